@@ -1,0 +1,189 @@
+"""CPU oracle, half-spectrum (r2c/c2r) restatement of the reference TGV time step.
+
+TEST INFRASTRUCTURE ONLY.  Nothing in the product path imports this module; only
+``tests/``, ``__graft_entry__.smoke()`` and the CPU legs of ``bench.py`` use it.
+
+Same numerics as :mod:`oracle.ref_c2c` (``src/ava_taylor_green_impl.hpp:658-1179`` of
+ovankerm/Spectral_solver) but the spectral state is stored on the half spectrum
+``mx in [0, N/2]`` with SciPy's pocketfft r2c/c2r (multithreaded through ``workers``),
+which makes 256^3 parity checks and the CPU baseline affordable.
+
+Why this is exact.  The reference consumes only the real part of every inverse transform
+(``:904-905, :1114, :1131, :1165``), i.e. it computes IDFT(H(c)) with H(c)_m =
+(c_m + conj(c_-m))/2.  Away from the planes mx = 0 and mx = N/2 the reference state is
+Hermitian, so H(c) = c there; pocketfft's c2r along x takes the real part of the mx = 0
+and mx = N/2 bins after the complex y/z inverse transforms, which is exactly H restricted
+to those planes.  The three self-conjugate Nyquist points (N/2,0,0), (0,N/2,0), (0,0,N/2)
+survive the sphere mask and carry complex values in the reference (``signed_mode`` maps
+index N/2 to +N/2, :123-125); the half spectrum stores each of them once, with its full
+complex value, so nothing is lost.  ``tests/test_oracle.py`` checks this module against
+the literal c2c restatement to round-off.
+
+Arrays are indexed ``[iz, iy, mx]`` (x fastest, as the reference layout).
+"""
+from __future__ import annotations
+
+import os
+
+import numpy as np
+import scipy.fft as sfft
+
+from .ref_c2c import PI, signed_mode
+
+WORKERS = int(os.environ.get("SNS_ORACLE_WORKERS", os.cpu_count() or 1))
+
+
+def half_mode_grids(n: int):
+    m = signed_mode(np.arange(n), n).astype(np.int64)
+    mxh = np.arange(n // 2 + 1, dtype=np.int64)  # index n/2 -> +n/2
+    return mxh[None, None, :], m[None, :, None], m[:, None, None]
+
+
+def full_to_half(c: np.ndarray) -> np.ndarray:
+    """Keep mx in [0, N/2] of a reference full spectrum (indexed [iz, iy, ix])."""
+    n = c.shape[-1]
+    return np.ascontiguousarray(c[..., : n // 2 + 1])
+
+
+def half_to_full(h: np.ndarray) -> np.ndarray:
+    """Rebuild the reference's full layout: mx < 0 from conj of the mirror mode."""
+    n = h.shape[0]
+    full = np.zeros((n, n, n), np.complex128)
+    full[..., : n // 2 + 1] = h
+    ix = np.arange(n // 2 + 1, n)
+    src = n - ix  # -mx
+    iy = (-np.arange(n)) % n
+    iz = (-np.arange(n)) % n
+    full[..., n // 2 + 1:] = np.conj(h[iz][:, iy][:, :, src])
+    return full
+
+
+class TaylorGreenR2C:
+    """Half-spectrum restatement of ``TaylorGreenSolver::Impl`` with identical numerics."""
+
+    def __init__(self, n: int, reynolds: float, u_hat0=None, workers: int | None = None):
+        if n <= 0:
+            raise ValueError("grid size must be positive")
+        if reynolds <= 0.0:
+            raise ValueError("Reynolds number must be positive")
+        self.n = n
+        self.nu = 1.0 / reynolds
+        self.global_size = n * n * n
+        self.workers = WORKERS if workers is None else workers
+        mx, my, mz = half_mode_grids(n)
+        msum = (mx + my + mz).astype(np.float64)
+        angle = (msum * PI) / float(n)  # initialize_metadata :782-783
+        self.phase = np.cos(angle) + 1j * np.sin(angle)
+        h = 0.5 * float(n)
+        m2 = (mx * mx + my * my + mz * mz).astype(np.float64)
+        self.keep = (m2 / (h * h)) <= 1.0  # keep_mode_host :131-134
+        self.k2 = m2
+        self.kvals = (mx.astype(np.float64), my.astype(np.float64), mz.astype(np.float64))
+        self.g = [None, None, None]
+        if u_hat0 is None:
+            self.initialize_velocity()
+        else:
+            self.u_hat = [np.array(c, np.complex128, copy=True) for c in u_hat0]
+
+    def forward(self, phys):
+        return sfft.rfftn(phys, workers=self.workers)
+
+    def backward_real(self, spec):
+        n = self.n
+        return sfft.irfftn(spec, s=(n, n, n), workers=self.workers)
+
+    def initialize_velocity(self):
+        n = self.n
+        i = np.arange(n, dtype=np.float64)
+        c = (i + 0.5) * 2.0 * PI / float(n)
+        x, y, z = c[None, None, :], c[None, :, None], c[:, None, None]
+        p0 = np.broadcast_to(np.sin(x) * np.cos(y) * np.cos(z), (n,) * 3)
+        p1 = np.broadcast_to(-np.cos(x) * np.sin(y) * np.cos(z), (n,) * 3)
+        p2 = np.zeros((n, n, n))
+        self.u_hat = [self.forward(np.ascontiguousarray(p)) for p in (p0, p1, p2)]
+        self.project_truncate(self.u_hat)
+
+    def project_truncate(self, f):
+        ix, iy, iz = self.kvals
+        k2 = self.k2
+        ok = (k2 > 0.0) & self.keep
+        inv = np.where(k2 > 0.0, 1.0 / np.where(k2 > 0.0, k2, 1.0), 0.0)
+        dot = (f[0] * ix + f[1] * iy) + f[2] * iz
+        factor = dot * inv
+        f[0][...] = np.where(ok, f[0] - factor * ix, 0.0)
+        f[1][...] = np.where(ok, f[1] - factor * iy, 0.0)
+        f[2][...] = np.where(ok, f[2] - factor * iz, 0.0)
+
+    def nonlinear(self, u_hat):
+        """Masked conservative-form nonlinear term only (before viscosity and projection)."""
+        phys = [self.backward_real(u) for u in u_hat]
+        shift = [self.backward_real(u * self.phase) for u in u_hat]
+        rhs = [np.zeros_like(u_hat[0]) for _ in range(3)]
+        kv = self.kvals
+        cphase = np.conj(self.phase)
+        for a, b in ((0, 0), (0, 1), (0, 2), (1, 1), (1, 2), (2, 2)):
+            c0 = self.forward(phys[a] * phys[b])
+            cs = self.forward(shift[a] * shift[b])
+            value = 0.5 * (c0 + cs * cphase)
+            value = np.where(self.keep, value, 0.0)
+            rhs[a] = rhs[a] + (-1j) * kv[b] * value
+            if a != b:
+                rhs[b] = rhs[b] + (-1j) * kv[a] * value
+        return rhs
+
+    def compute_rhs(self, u_hat=None):
+        if u_hat is None:
+            u_hat = self.u_hat
+        rhs = self.nonlinear(u_hat)
+        for c in range(3):
+            rhs[c] = rhs[c] - u_hat[c] * (self.nu * self.k2)
+        self.project_truncate(rhs)
+        return rhs
+
+    def step(self, dt: float):
+        u, g = self.u_hat, self.g
+        r = self.compute_rhs()
+        for c in range(3):
+            g[c] = r[c].copy()
+            u[c] = u[c] + g[c] * (dt / 3.0)
+        self.project_truncate(u)
+        r = self.compute_rhs()
+        for c in range(3):
+            g[c] = g[c] * (-5.0 / 9.0) + r[c]
+            u[c] = u[c] + g[c] * (15.0 * dt / 16.0)
+        self.project_truncate(u)
+        r = self.compute_rhs()
+        for c in range(3):
+            g[c] = g[c] * (-153.0 / 128.0) + r[c]
+            u[c] = u[c] + g[c] * (8.0 * dt / 15.0)
+        self.project_truncate(u)
+
+    step_rk3 = step
+
+    def velocity(self):
+        return [self.backward_real(u) for u in self.u_hat]
+
+    def max_velocity(self) -> float:
+        p = self.velocity()
+        return float(np.sqrt(np.max(p[0] * p[0] + p[1] * p[1] + p[2] * p[2])))
+
+    def vorticity_hat(self, u):
+        ix, iy, iz = self.kvals
+        return [1j * (iy * u[2] - iz * u[1]), 1j * (iz * u[0] - ix * u[2]), 1j * (ix * u[1] - iy * u[0])]
+
+    def diagnostics(self, t: float) -> dict:
+        u = self.u_hat
+        p = [self.backward_real(c) for c in u]
+        s2 = p[0] * p[0] + p[1] * p[1] + p[2] * p[2]
+        energy = float(np.sum(0.5 * s2)) / self.global_size
+        vmax2 = float(np.max(s2))
+        w = [self.backward_real(c) for c in self.vorticity_hat(u)]
+        enstrophy = float(np.sum(0.5 * (w[0] * w[0] + w[1] * w[1] + w[2] * w[2]))) / self.global_size
+        ix, iy, iz = self.kvals
+        div = (u[0] * ix + u[1] * iy) + u[2] * iz
+        maxdiv = float(np.max(np.sqrt(div.real * div.real + div.imag * div.imag)))
+        return dict(t=t, kinetic_energy=energy, dissipation=2.0 * self.nu * enstrophy,
+                    enstrophy=enstrophy, max_spectral_divergence=maxdiv, max_velocity=float(np.sqrt(vmax2)))
+
+    def get_state_full(self):
+        return [half_to_full(c) for c in self.u_hat]
