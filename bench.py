@@ -1,0 +1,304 @@
+#!/usr/bin/env python
+"""Benchmark of the pseudo-spectral Taylor-Green RK3 step on B200.
+
+Workload (one "step" = one low-storage RK3 step over the whole grid): Taylor-Green vortex,
+N = 512^3, FP64 plain form (the reference's scheme: phase-shift dealiasing, sphere
+truncation, explicit viscosity, Williamson RK3), Re = 1600, dt = 1e-3.  The state stays
+resident in HBM (19.9 GB, far above the 126 MB L2, so no L2 flush is needed).
+
+Metric: grid-point * RK3-steps per second, in units of 1e9 (Gpt*RK3-steps/s).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--n 512]
+
+With --gpus N > 1 (torchrun, one rank per GPU) every rank steps its own replica (the
+path does not shard without an all-to-all transpose, so multi-GPU is replicas only);
+`value` is the sum over ranks divided by the slowest rank's device time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "512³ Gpt·RK3-steps/s mixed vs FP64 plain at ε≤1e-6; served solves/s, p50/p99"
+UNIT = "Gpt*RK3-steps/s"
+RE = 1600.0
+DT = 1e-3
+
+# Algorithmic bytes per launch of each pass, in units of S = N^3 * 8 B (one FP64 real field
+# or one half-spectrum complex field): every field read or written once.
+PASS_BYTES_S = {"zpass_inv_phase": 9, "ypass_inv": 12, "xpass_products": 18, "nyq_reduce": 0,
+                "ypass_fwd": 24, "zpass_fwd": 24, "sweep": 23}
+LAUNCHES_PER_STEP = 3 * 7
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if self.proc is None or self.path is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        rows = []
+        with open(self.path) as f:
+            for line in f:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        pg = dist
+    return world, rank, local, pg
+
+
+def barrier_sync(pg):
+    import torch
+    torch.cuda.synchronize()
+    if pg is not None:
+        pg.barrier()
+    torch.cuda.synchronize()
+
+
+def max_over_ranks(pg, value: float) -> float:
+    if pg is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def cpu_oracle_rate(n: int, sample_stages: int = 1):
+    """Time the CPU oracle (half-spectrum restatement, scipy pocketfft with every host
+    thread) on `sample_stages` RK3 stages at N^3; returns (Gpt*steps/s, seconds, threads)."""
+    from oracle import ref_r2c
+    threads = os.cpu_count() or 1
+    s = ref_r2c.TaylorGreenR2C(n, RE, workers=threads)
+    s.g = [None, None, None]
+    t0 = time.perf_counter()
+    for _ in range(sample_stages):
+        r = s.compute_rhs()
+        for c in range(3):
+            s.g[c] = r[c]
+            s.u_hat[c] = s.u_hat[c] + s.g[c] * (DT / 3.0)
+        s.project_truncate(s.u_hat)
+    dt = time.perf_counter() - t0
+    steps = sample_stages / 3.0
+    return n ** 3 * steps / dt / 1e9, dt, threads
+
+
+def run_reference(args, world, rank, pg):
+    """--impl reference: the reference's CPU path on the host cores.  The reference itself
+    cannot be built here (FFTW3, MPI, AVA and FLUPS are absent), so its CPU restatement
+    (the oracle) is what runs."""
+    if rank != 0:
+        return 0
+    n = args.n
+    # warm-up: the code paths and pocketfft plans on a small grid (a 512^3 stage is ~30 s)
+    for _ in range(max(1, min(args.warmup, 3))):
+        cpu_oracle_rate(64, 1)
+    # each timed "step" is one RK3 stage at N^3; capped so the arm ends within minutes
+    k = max(1, min(args.steps, 4 if n >= 512 else args.steps))
+    total_s = 0.0
+    threads = os.cpu_count() or 1
+    for _ in range(k):
+        _, s, threads = cpu_oracle_rate(n, 1)
+        total_s += s
+    units = n ** 3 * (k / 3.0)
+    value = units / total_s / 1e9
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": k, "warmup": args.warmup, "ms_per_step": 3 * 1e3 * total_s / k,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic: analytic Taylor-Green initial field",
+        "config": {"workload": f"Taylor-Green RK3, {n}^3, FP64 plain, Re=1600, dt=1e-3", "n": n,
+                   "precision": "fp64", "each_step": "one RK3 stage (1/3 step) of the CPU oracle"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"{k} RK3 stages at {n}^3 (oracle/ref_r2c.py, scipy pocketfft, "
+                                   f"{threads} threads); reference FFTW path unbuildable here"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_b200(args, world, rank, local, pg):
+    import numpy as np
+    import torch
+    from spectral_solver_b200 import Solver
+
+    n = args.n
+    torch.cuda.set_device(local)
+    s = Solver(n, RE)
+    # warm-up (untimed)
+    s.step(DT, args.warmup)
+    barrier_sync(pg)
+    with ClockSampler(local) as clk:
+        ms = s.time_steps(DT, args.steps)  # CUDA events on the library's launching stream
+    barrier_sync(pg)
+    clocks = clk.summary()
+    ms_max = max_over_ranks(pg, ms)
+    units = world * n ** 3 * args.steps
+    value = units / (ms_max / 1e3) / 1e9
+
+    # Per-pass device times (events between passes, separate from the timed region).
+    prof = s.profile_passes(DT, 1)
+    S = n ** 3 * 8
+    top = max(prof, key=prof.get)
+    achieved = PASS_BYTES_S[top] * S / (prof[top] / 1e3) / 1e9
+    peak, peak_kind = load_peaks()
+
+    # End to end through the C ABI with host buffers: upload the initial spectral state from
+    # pinned host memory, K steps each followed by a diagnostics row read back to the host,
+    # then the final physical velocity read back -- a whole solve from the user's side.
+    state = s.get_state()
+    pin = [torch.empty(2 * n ** 3, dtype=torch.float64, pin_memory=True) for _ in range(3)]
+    for c in range(3):
+        pin[c].numpy()[:] = state[c].view(np.float64).reshape(-1)
+    out = [torch.empty(n ** 3, dtype=torch.float64, pin_memory=True) for _ in range(3)]
+    import ctypes as C
+    from spectral_solver_b200 import _lib
+    lib = _lib.load()
+    DP = C.POINTER(C.c_double)
+    ins = (DP * 3)(*[C.cast(p.data_ptr(), DP) for p in pin])
+    outs = (DP * 3)(*[C.cast(p.data_ptr(), DP) for p in out])
+    diag = _lib.SnsDiag()
+    barrier_sync(pg)
+    t0 = time.perf_counter()
+    rc = lib.sns_set_state(s.h, ins)
+    t = 0.0
+    for _ in range(args.steps):
+        rc |= lib.sns_step(s.h, DT, 1)
+        t += DT
+        rc |= lib.sns_diagnostics(s.h, t, C.byref(diag))
+    rc |= lib.sns_dump_velocity(s.h, outs)
+    e2e_s = time.perf_counter() - t0
+    if rc != 0:
+        raise RuntimeError("e2e run failed: " + lib.sns_last_error(s.h).decode())
+    e2e_s = max_over_ranks(pg, e2e_s)
+    e2e_value = units / e2e_s / 1e9
+    h2d = 3 * 2 * n ** 3 * 8 / args.steps
+    d2h = (3 * n ** 3 * 8 + args.steps * 4 * 8) / args.steps
+    s.close()
+
+    if rank == 0:
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            rate, secs, threads = cpu_oracle_rate(n, 1)
+            cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
+                   "sample": f"1 RK3 stage at {n}^3 ({secs:.1f} s) of the CPU oracle (oracle/ref_r2c.py, scipy "
+                             f"pocketfft, {threads} threads); the reference's FFTW path cannot be built here"}
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic: analytic Taylor-Green initial field (Re=1600)",
+            "config": {"workload": f"Taylor-Green RK3 step, {n}^3, FP64 plain drop-in form "
+                                   "(phase-shift dealiasing, sphere truncation, explicit viscosity)",
+                       "n": n, "precision": "fp64", "reynolds": RE, "dt": DT,
+                       "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
+                       "l2": f"inputs larger than L2 ({(18 * n * n * (((n // 2 + 1) + 7) // 8 * 8) * 16) / 1e9:.1f} GB resident)"},
+            "clocks": clocks,
+            "gpu_launches": LAUNCHES_PER_STEP * args.steps,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None, "kernel": top,
+                         "peak_source": f"hbm_gbs {peak_kind}",
+                         "algorithmic_bytes_per_launch": PASS_BYTES_S[top] * S,
+                         "mean_launch_ms": prof[top]},
+            "passes_ms_per_stage": prof,
+            "model_roofline_frac": value / (peak / (261 * 8)),
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "what": "set_state from pinned host + K x (step + diagnostics row to host) + final velocity to host"},
+        }
+        if cpu is not None:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--n", type=int, default=512)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        # CPU-only arm: no process group; under torchrun rank 0 alone runs
+        return run_reference(args, int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), None)
+    world, rank, local, pg = dist_setup(args)
+    try:
+        return run_b200(args, world, rank, local, pg)
+    finally:
+        if pg is not None:
+            pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    sys.exit(main())

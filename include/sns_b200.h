@@ -1,0 +1,124 @@
+/* sns_b200.h — C ABI of the B200 pseudo-spectral Taylor-Green solver (libsns_b200.so).
+ *
+ * Plain pointers and sizes only.  Every entry point returns SNS_OK (0) or an SNS_ERR_*
+ * code; no C++ exception crosses this boundary; sns_last_error() gives the message.
+ * A handle owns all its device memory and one CUDA stream on the device that was current
+ * when it was created.  Calls are synchronous on that stream (they return after the GPU
+ * work finished).  One handle per host thread: there is no internal locking.
+ *
+ * Layouts on the host side are the reference's (ovankerm/Spectral_solver):
+ *   physical field: N^3 doubles, x fastest, id = ix + N*(iy + N*iz)
+ *                   (FftwFft3D::for_each_physical, src/fftw_fft.hpp:30-40);
+ *   spectral field: 2*N^3 doubles, interleaved complex, same index order, mode
+ *                   m = i <= N/2 ? i : i - N on each axis (fftw_fft.hpp:45-71).
+ * On the device the spectra live on the half spectrum mx in [0, N/2].
+ *
+ * Supported N: 8, 12, 16, 24, 32, 48, 64, 96, 128, 256, 512 (radix-2/3/4/8 plans);
+ * domain [0, 2*pi)^3 so the wavenumber equals the integer mode.
+ */
+#ifndef SNS_B200_H
+#define SNS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  SNS_OK = 0,
+  SNS_ERR_INVALID = 1,        /* bad argument (null pointer, non-positive Re, ...) */
+  SNS_ERR_UNSUPPORTED = 2,    /* grid size without an FFT plan, or mode not built */
+  SNS_ERR_CUDA = 3,           /* CUDA runtime error (message has the CUDA string) */
+  SNS_ERR_NOMEM = 4,          /* device allocation failed or exceeds the HBM budget */
+  SNS_ERR_NO_DEVICE = 5,      /* no CUDA device visible */
+  SNS_ERR_INJECTED = 6        /* failure forced by sns_debug_fail_after (tests only) */
+};
+
+enum { SNS_PRECISION_FP64 = 0 };
+enum { SNS_VISCOUS_EXPLICIT = 0 };
+
+typedef struct sns_handle sns_handle;
+
+/* Diagnostics row, the reference's Diagnostics (src/ava_taylor_green.hpp:8-19) minus the
+ * run-loop columns (dt, cfl, main_dt, main_cfl), which the driver fills. */
+typedef struct sns_diag {
+  double t;
+  double kinetic_energy;
+  double dissipation;
+  double enstrophy;
+  double max_spectral_divergence;
+  double max_velocity;
+} sns_diag;
+
+/* Library version string. */
+const char* sns_version(void);
+
+/* Bytes of device memory a solver handle of size n needs (state + work + tables). */
+size_t sns_bytes_required(int n, int precision);
+
+/* Create a solver: Taylor-Green initial field (u = sin x cos y cos z, v = -cos x sin y cos z,
+ * w = 0 at cell centres), plus, if pert_amp > 0, the seeded solenoidal k^(-5/3)
+ * perturbation with 1 <= |m| <= pert_kmax scaled to rms |u'| = pert_amp; then the Leray
+ * projection and sphere truncation.  nu = 1/Re.
+ * Replaces TaylorGreenSolver::TaylorGreenSolver(int n, double reynolds)
+ * (src/ava_taylor_green.hpp:40, impl :703-716); errors as its std::runtime_error. */
+int sns_create(int n, double nu, int precision, int viscous_mode, uint64_t seed, double pert_amp, int pert_kmax,
+               sns_handle** out);
+int sns_destroy(sns_handle* h);
+
+/* Message of the last failed call on h (or of the last failed sns_create when h is NULL). */
+const char* sns_last_error(const sns_handle* h);
+
+/* FFT-backend contract (FftwFft3D::forward / backward, src/fftw_fft.cpp:53-85):
+ * forward: N^3 real -> 2*N^3 doubles, unnormalised, sign -1;
+ * backward: 2*N^3 doubles -> N^3 real = Re(IDFT(c)) / N^3 for any input, Hermitian or not. */
+int sns_forward_r2c(sns_handle* h, const double* host_physical, double* host_spectral);
+int sns_backward_c2r(sns_handle* h, const double* host_spectral, double* host_physical);
+
+/* State exchange in the reference's full complex layout (3 arrays of 2*N^3 doubles).
+ * set_state keeps mx in [0, N/2]; the rest of a reference state is its conjugate mirror. */
+int sns_set_state(sns_handle* h, const double* const uhat_full[3]);
+int sns_get_state(sns_handle* h, double* const uhat_full[3]);
+
+/* Projected right-hand side of the reference's compute_rhs (ava_taylor_green_impl.hpp:847-977)
+ * for the given state (full layout in and out).  The handle's own state is not changed. */
+int sns_rhs(sns_handle* h, const double* const uhat_full[3], double* const rhs_full[3]);
+
+/* nsteps Williamson RK3 steps of size dt (TaylorGreenSolver::step_rk3, :979-1045). */
+int sns_step(sns_handle* h, double dt, int nsteps);
+
+/* Diagnostics of the current state (TaylorGreenSolver::diagnostics, :1122-1179) and the
+ * maximum velocity magnitude (TaylorGreenSolver::max_velocity, :1105-1120). */
+int sns_diagnostics(sns_handle* h, double t, sns_diag* out);
+int sns_max_velocity(sns_handle* h, double* out);
+
+/* Final physical velocity: 3 arrays of N^3 doubles (the reference's layout). */
+int sns_dump_velocity(sns_handle* h, double* const phys[3]);
+
+/* Grid size and device bytes held by the handle. */
+int sns_grid_size(const sns_handle* h);
+size_t sns_device_bytes(const sns_handle* h);
+
+/* Time `nsteps` steps on the device with CUDA events (no host copies); writes the elapsed
+ * milliseconds.  Used by the benchmark; the state advances as with sns_step. */
+int sns_time_steps(sns_handle* h, double dt, int nsteps, double* elapsed_ms);
+
+/* Per-pass device time: runs nsteps steps (the state advances) with CUDA events between
+ * the passes of every stage on the handle's stream and writes the mean milliseconds per
+ * stage of each pass into pass_ms[SNS_NUM_PASSES], in the order
+ * inverse z (+phase), inverse y, fused x (products), Nyquist sums, forward y, forward z,
+ * k-space sweep.  Benchmark/profiling aid; not for timed runs. */
+#define SNS_NUM_PASSES 7
+int sns_profile_passes(sns_handle* h, double dt, int nsteps, double* pass_ms);
+
+/* Test hook: the k-th following call into the handle fails with SNS_ERR_INJECTED
+ * (k <= 0 disables).  Exercises the error paths without touching the GPU. */
+int sns_debug_fail_after(sns_handle* h, int k);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SNS_B200_H */

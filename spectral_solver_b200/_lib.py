@@ -1,0 +1,209 @@
+"""ctypes binding of the C ABI in ``include/sns_b200.h`` (``libsns_b200.so``).
+
+The library is built in-tree (``spectral_solver_b200/build.py``); loading fails loudly if
+it is missing — there is no fallback implementation.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_PKG, "libsns_b200.so")
+
+SNS_OK = 0
+SNS_ERR_INVALID = 1
+SNS_ERR_UNSUPPORTED = 2
+SNS_ERR_CUDA = 3
+SNS_ERR_NOMEM = 4
+SNS_ERR_NO_DEVICE = 5
+SNS_ERR_INJECTED = 6
+PRECISION_FP64 = 0
+VISCOUS_EXPLICIT = 0
+
+# Every symbol include/sns_b200.h declares, with its ctypes signature.
+_DP = C.POINTER(C.c_double)
+_DPP = C.POINTER(_DP)
+_H = C.c_void_p
+
+
+class SnsDiag(C.Structure):
+    _fields_ = [("t", C.c_double), ("kinetic_energy", C.c_double), ("dissipation", C.c_double),
+                ("enstrophy", C.c_double), ("max_spectral_divergence", C.c_double),
+                ("max_velocity", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+SIGNATURES = {
+    "sns_version": (C.c_char_p, []),
+    "sns_bytes_required": (C.c_size_t, [C.c_int, C.c_int]),
+    "sns_create": (C.c_int, [C.c_int, C.c_double, C.c_int, C.c_int, C.c_uint64, C.c_double, C.c_int,
+                             C.POINTER(_H)]),
+    "sns_destroy": (C.c_int, [_H]),
+    "sns_last_error": (C.c_char_p, [_H]),
+    "sns_forward_r2c": (C.c_int, [_H, _DP, _DP]),
+    "sns_backward_c2r": (C.c_int, [_H, _DP, _DP]),
+    "sns_set_state": (C.c_int, [_H, _DPP]),
+    "sns_get_state": (C.c_int, [_H, _DPP]),
+    "sns_rhs": (C.c_int, [_H, _DPP, _DPP]),
+    "sns_step": (C.c_int, [_H, C.c_double, C.c_int]),
+    "sns_diagnostics": (C.c_int, [_H, C.c_double, C.POINTER(SnsDiag)]),
+    "sns_max_velocity": (C.c_int, [_H, _DP]),
+    "sns_dump_velocity": (C.c_int, [_H, _DPP]),
+    "sns_grid_size": (C.c_int, [_H]),
+    "sns_device_bytes": (C.c_size_t, [_H]),
+    "sns_time_steps": (C.c_int, [_H, C.c_double, C.c_int, _DP]),
+    "sns_debug_fail_after": (C.c_int, [_H, C.c_int]),
+    "sns_profile_passes": (C.c_int, [_H, C.c_double, C.c_int, _DP]),
+}
+
+PASS_NAMES = ("zpass_inv_phase", "ypass_inv", "xpass_products", "nyq_reduce", "ypass_fwd", "zpass_fwd", "sweep")
+
+_lib = None
+
+
+def load(path: str = LIB_PATH):
+    """Load libsns_b200.so and attach signatures.  Raises if it was not built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise RuntimeError(f"{path} is missing: run __graft_entry__.build() (no CPU fallback exists)")
+    lib = C.CDLL(path)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+class SnsError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+
+
+def _dptr(a: np.ndarray):
+    assert a.dtype == np.float64 and a.flags.c_contiguous
+    return a.ctypes.data_as(_DP)
+
+
+def _arr3(arrs):
+    return (_DP * 3)(*[_dptr(a) for a in arrs])
+
+
+def full_to_interleaved(c: np.ndarray) -> np.ndarray:
+    """complex [iz, iy, ix] -> 2*N^3 doubles (the reference's interleaved storage)."""
+    return np.ascontiguousarray(c, dtype=np.complex128).view(np.float64).reshape(-1)
+
+
+def interleaved_to_full(d: np.ndarray, n: int) -> np.ndarray:
+    return d.view(np.complex128).reshape(n, n, n)
+
+
+class Solver:
+    """Thin RAII wrapper of an ``sns_handle`` (Python mirror of TaylorGreenSolver)."""
+
+    def __init__(self, n: int, reynolds: float = 1600.0, seed: int = 0, pert_amp: float = 0.0,
+                 pert_kmax: int = 0, nu: float | None = None):
+        self.lib = load()
+        self.n = n
+        self.nu = (1.0 / reynolds) if nu is None else nu
+        h = _H()
+        rc = self.lib.sns_create(n, self.nu, PRECISION_FP64, VISCOUS_EXPLICIT, seed, pert_amp, pert_kmax,
+                                 C.byref(h))
+        if rc != SNS_OK:
+            raise SnsError(rc, self.lib.sns_last_error(None).decode())
+        self.h = h
+
+    def _check(self, rc):
+        if rc != SNS_OK:
+            raise SnsError(rc, self.lib.sns_last_error(self.h).decode())
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.sns_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # FFT-backend contract
+    def forward(self, phys: np.ndarray) -> np.ndarray:
+        n = self.n
+        x = np.ascontiguousarray(phys, dtype=np.float64).reshape(-1)
+        out = np.empty(2 * n ** 3, np.float64)
+        self._check(self.lib.sns_forward_r2c(self.h, _dptr(x), _dptr(out)))
+        return interleaved_to_full(out, n)
+
+    def backward(self, spec: np.ndarray) -> np.ndarray:
+        n = self.n
+        x = full_to_interleaved(spec)
+        out = np.empty(n ** 3, np.float64)
+        self._check(self.lib.sns_backward_c2r(self.h, _dptr(x), _dptr(out)))
+        return out.reshape(n, n, n)
+
+    def set_state(self, u_full):
+        arrs = [full_to_interleaved(c) for c in u_full]
+        self._check(self.lib.sns_set_state(self.h, _arr3(arrs)))
+
+    def get_state(self):
+        n = self.n
+        arrs = [np.empty(2 * n ** 3, np.float64) for _ in range(3)]
+        self._check(self.lib.sns_get_state(self.h, _arr3(arrs)))
+        return [interleaved_to_full(a, n) for a in arrs]
+
+    def rhs(self, u_full):
+        n = self.n
+        ins = [full_to_interleaved(c) for c in u_full]
+        outs = [np.empty(2 * n ** 3, np.float64) for _ in range(3)]
+        self._check(self.lib.sns_rhs(self.h, _arr3(ins), _arr3(outs)))
+        return [interleaved_to_full(a, n) for a in outs]
+
+    def step(self, dt: float, nsteps: int = 1):
+        self._check(self.lib.sns_step(self.h, dt, nsteps))
+
+    step_rk3 = step
+
+    def time_steps(self, dt: float, nsteps: int) -> float:
+        ms = C.c_double()
+        self._check(self.lib.sns_time_steps(self.h, dt, nsteps, C.byref(ms)))
+        return ms.value
+
+    def diagnostics(self, t: float = 0.0) -> dict:
+        d = SnsDiag()
+        self._check(self.lib.sns_diagnostics(self.h, t, C.byref(d)))
+        return d.as_dict()
+
+    def max_velocity(self) -> float:
+        v = C.c_double()
+        self._check(self.lib.sns_max_velocity(self.h, C.byref(v)))
+        return v.value
+
+    def dump_velocity(self):
+        n = self.n
+        arrs = [np.empty(n ** 3, np.float64) for _ in range(3)]
+        self._check(self.lib.sns_dump_velocity(self.h, _arr3(arrs)))
+        return [a.reshape(n, n, n) for a in arrs]
+
+    def profile_passes(self, dt: float, nsteps: int) -> dict:
+        out = (C.c_double * len(PASS_NAMES))()
+        self._check(self.lib.sns_profile_passes(self.h, dt, nsteps, out))
+        return dict(zip(PASS_NAMES, list(out)))
+
+    def device_bytes(self) -> int:
+        return int(self.lib.sns_device_bytes(self.h))

@@ -1,0 +1,643 @@
+// C ABI of the B200 Taylor-Green solver: handle, device memory, tables, step orchestration.
+//
+// Device memory of a handle (FP64 plain form), in half fields of N*N*pitch double2:
+//   state : u[3], g[3]            (the reference's u_hat and g, ava_taylor_green_impl.hpp:665-667)
+//   work  : 12 fields             (inverse-transformed velocity on both grids, then the
+//                                  12 product spectra; the fused x pass reads 6 and writes
+//                                  12 rows in place, so one buffer serves both)
+//   tables: twiddles (N), phase exp(i*pi*(mx+my+mz)/N) for mx+my+mz in [-3N/2, 3N/2],
+//           reduction partials, the 12 Nyquist-plane sums.
+#include "sns_kernels.cuh"
+#include "../../include/sns_b200.h"
+
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <exception>
+#include <new>
+#include <string>
+#include <vector>
+
+namespace {
+
+constexpr double kPi = 3.141592653589793238462643383279502884;
+
+struct SnsError : std::exception {
+  int code;
+  std::string msg;
+  SnsError(int c, std::string m) : code(c), msg(std::move(m)) {}
+  const char* what() const noexcept override { return msg.c_str(); }
+};
+
+void ck(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) throw SnsError(SNS_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+thread_local std::string g_create_error;
+
+}  // namespace
+
+struct sns_handle {
+  int n = 0;
+  int device = 0;
+  double nu = 0.0;
+  int precision = 0;
+  int viscous_mode = 0;
+  sns::Geom g{};
+  const sns::Ops* ops = nullptr;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  double2* state = nullptr;  // u[3] then g[3]
+  double2* work = nullptr;   // 12 fields
+  double2* tw = nullptr;
+  double2* phase = nullptr;
+  double* partials = nullptr;
+  double* nyqsum = nullptr;
+  double* red = nullptr;  // reduction results
+  size_t partial_count = 0;
+  size_t bytes = 0;
+  int fail_after = 0;
+  // true when the state's mx = N/2 plane is zero off (N/2,0,0), as every masked state is;
+  // then the passes skip that column and take the Nyquist mode from the state directly
+  bool nyq_clean = true;
+  std::string err;
+
+  double2* u() const { return state; }
+  double2* gb() const { return state + 3 * g.field; }
+  double2* wf(int i) const { return work + (long long)i * g.field; }
+  int tiles_data() const { return (g.nh + 7) / 8; }   // columns [0, N/2)
+  int tiles_all() const { return g.pitch / 8; }        // Nyquist column included
+  double inv_size() const { return 1.0 / ((double)n * n * n); }
+};
+
+namespace {
+
+size_t field_bytes(int n) { return (size_t)n * n * sns::pitch_for(n) * sizeof(double2); }
+
+size_t partial_slots(int n) {
+  const size_t rows = (size_t)n * n;
+  return 2 * rows + 4096;
+}
+
+// exp(-2*pi*i*t/L) rounded from long double; exact at the quarter points.
+std::vector<double2> twiddle_table(int L) {
+  std::vector<double2> tw(L);
+  for (int t = 0; t < L; ++t) {
+    const int q = (4 * t) % (4 * L);
+    if (q % L == 0) {
+      const int k = q / L;  // t*4/L in {0,1,2,3}
+      const double c[4] = {1.0, 0.0, -1.0, 0.0};
+      const double s[4] = {0.0, -1.0, 0.0, 1.0};
+      tw[t] = make_double2(c[k], s[k]);
+    } else {
+      const long double a = -2.0L * 3.141592653589793238462643383279502884L * (long double)t / (long double)L;
+      tw[t] = make_double2((double)cosl(a), (double)sinl(a));
+    }
+  }
+  return tw;
+}
+
+// Phase table computed exactly as the reference does on the host
+// (initialize_metadata, ava_taylor_green_impl.hpp:782-783): angle = (msum * pi) / n.
+std::vector<double2> phase_table(int n) {
+  std::vector<double2> ph(3 * n + 1);
+  for (int i = 0; i <= 3 * n; ++i) {
+    const int msum = i - 3 * n / 2;
+    const double angle = (static_cast<double>(msum) * kPi) / static_cast<double>(n);
+    ph[i] = make_double2(std::cos(angle), std::sin(angle));
+  }
+  return ph;
+}
+
+uint64_t splitmix64(uint64_t x) {
+  uint64_t z = x + 0x9E3779B97F4A7C15ULL;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+  return z ^ (z >> 31);
+}
+
+
+// Seeded solenoidal k^(-5/3) perturbation (the project's own specification; the reference
+// starts from the pure Taylor-Green field).  Returns sparse (index, value) entries in the
+// half layout of the 3 consecutive state fields.
+void perturbation_entries(int n, uint64_t seed, double amp, int kmax, const sns::Geom& g,
+                          std::vector<long long>& idx, std::vector<double2>& val) {
+  idx.clear();
+  val.clear();
+  if (amp == 0.0 || kmax < 1) return;
+  if (2 * kmax >= n) throw SnsError(SNS_ERR_INVALID, "perturbation kmax must be below N/2");
+  struct Mode { int mx, my, mz; double v[6]; };
+  std::vector<Mode> modes;
+  const uint64_t h = splitmix64(seed);
+  double total = 0.0;
+  for (int mz = -kmax; mz <= kmax; ++mz)
+    for (int my = -kmax; my <= kmax; ++my)
+      for (int mx = 0; mx <= kmax; ++mx) {
+        const int k2 = mx * mx + my * my + mz * mz;
+        if (k2 < 1 || k2 > kmax * kmax) continue;
+        const bool canon = mx > 0 || my > 0 || (my == 0 && mz > 0);
+        if (!canon) continue;
+        const uint64_t flat = (uint64_t)mx + (uint64_t)n * ((uint64_t)((my % n + n) % n) +
+                                                            (uint64_t)n * (uint64_t)((mz % n + n) % n));
+        const double kk = (double)k2;
+        const double a = std::pow(std::sqrt(kk), -5.0 / 3.0);
+        double re[3], im[3];
+        for (int c = 0; c < 3; ++c) {
+          const uint64_t r = splitmix64(h ^ (3ULL * flat + (uint64_t)c));
+          const double theta = (double)(r >> 11) * (1.0 / 9007199254740992.0);
+          const double ang = 2.0 * kPi * theta;
+          re[c] = a * std::cos(ang);
+          im[c] = a * std::sin(ang);
+        }
+        const double fx = mx, fy = my, fz = mz;
+        const double dre = (re[0] * fx + re[1] * fy) + re[2] * fz;
+        const double dim = (im[0] * fx + im[1] * fy) + im[2] * fz;
+        const double kv[3] = {fx, fy, fz};
+        Mode m{mx, my, mz, {}};
+        for (int c = 0; c < 3; ++c) {
+          m.v[2 * c] = re[c] - (dre / kk) * kv[c];
+          m.v[2 * c + 1] = im[c] - (dim / kk) * kv[c];
+          total += 2.0 * (m.v[2 * c] * m.v[2 * c] + m.v[2 * c + 1] * m.v[2 * c + 1]);
+        }
+        modes.push_back(m);
+      }
+  const double n6 = std::pow((double)n, 6.0);
+  const double s = amp / std::sqrt(total / n6);
+  for (const Mode& m : modes) {
+    const long long row = (long long)((m.mz % n + n) % n) * n + ((m.my % n + n) % n);
+    for (int c = 0; c < 3; ++c) {
+      idx.push_back((long long)c * g.field + row * g.pitch + m.mx);
+      val.push_back(make_double2(m.v[2 * c] * s, m.v[2 * c + 1] * s));
+      if (m.mx == 0) {
+        const long long rowm = (long long)(((-m.mz) % n + n) % n) * n + (((-m.my) % n + n) % n);
+        idx.push_back((long long)c * g.field + rowm * g.pitch);
+        val.push_back(make_double2(m.v[2 * c] * s, -m.v[2 * c + 1] * s));
+      }
+    }
+  }
+}
+
+void check_inject(sns_handle* h) {
+  if (h->fail_after > 0) {
+    if (--h->fail_after == 0) throw SnsError(SNS_ERR_INJECTED, "failure injected by sns_debug_fail_after");
+  }
+}
+
+void sync(sns_handle* h, const char* what) {
+  ck(cudaGetLastError(), what);
+  ck(cudaStreamSynchronize(h->stream), what);
+}
+
+// Optional per-pass event marks (profiling entry point only).
+struct PassMarks {
+  cudaEvent_t ev[8];
+  bool on = false;
+};
+
+inline void mark(PassMarks* pm, int i, cudaStream_t st) {
+  if (pm && pm->on) cudaEventRecord(pm->ev[i], st);
+}
+
+// One RK3 stage (or the RHS only, mode 1) on u_src: the five fused passes.
+void run_stage(sns_handle* h, double2* u_src, double2* g_buf, int stage, double dt, int mode, double2* rhs_out,
+               double* partials, PassMarks* pm = nullptr) {
+  const sns::Ops* o = h->ops;
+  const sns::Geom& g = h->g;
+  cudaStream_t st = h->stream;
+  const int tiles_in = h->nyq_clean ? h->tiles_data() : h->tiles_all();
+  mark(pm, 0, st);
+  o->zpass_inv_phase(u_src, h->work, h->tw, h->phase, h->inv_size(), tiles_in, g, st);
+  mark(pm, 1, st);
+  o->ypass(h->work, 6, +1, tiles_in, h->tw, g, st);
+  mark(pm, 2, st);
+  o->xpass_products(h->work, u_src, h->phase, h->inv_size(), h->nyq_clean ? 1 : 0, partials, h->tw, g, st);
+  mark(pm, 3, st);
+  o->nyq_reduce(h->work, h->nyqsum, g, st);
+  mark(pm, 4, st);
+  o->ypass(h->work, 12, -1, h->tiles_data(), h->tw, g, st);
+  mark(pm, 5, st);
+  o->zpass(h->work, h->work, 12, -1, h->tiles_data(), 1.0, h->tw, g, st);
+  mark(pm, 6, st);
+  sns::SweepArgs a{};
+  a.nu = h->nu;
+  a.stage = stage;
+  a.mode = mode;
+  a.dealias = 1;
+  if (stage == 0) {
+    a.ga = 0.0;
+    a.ub = dt / 3.0;
+  } else if (stage == 1) {
+    a.ga = -5.0 / 9.0;
+    a.ub = 15.0 * dt / 16.0;
+  } else {
+    a.ga = -153.0 / 128.0;
+    a.ub = 8.0 * dt / 15.0;
+  }
+  o->sweep(h->work, u_src, g_buf, rhs_out, h->nyqsum, h->phase, a, g, st);
+  mark(pm, 7, st);
+}
+
+void step_once(sns_handle* h, double dt) {
+  for (int s = 0; s < 3; ++s) {
+    run_stage(h, h->u(), h->gb(), s, dt, 0, nullptr, nullptr);
+    h->nyq_clean = true;  // the sweep zeroes the plane mx = N/2 off (N/2,0,0)
+  }
+}
+
+// Does a reference full-layout spectrum carry content on the plane mx = N/2 off (N/2,0,0)?
+bool nyquist_plane_dirty(int n, const double* full) {
+  const int nh = n / 2;
+  for (long long z = 0; z < n; ++z)
+    for (long long y = 0; y < n; ++y) {
+      if (y == 0 && z == 0) continue;
+      const double* v = full + 2 * ((z * n + y) * n + nh);
+      if (v[0] != 0.0 || v[1] != 0.0) return true;
+    }
+  return false;
+}
+
+// Upload a reference full-layout field into half field `dst` (optionally Hermitian part).
+void upload_full(sns_handle* h, const double* host, double2* dst, int herm) {
+  double2* staging = h->wf(4);  // N^3 double2 fit in work fields 4..(4 + N/pitch)
+  const size_t bytes = (size_t)h->n * h->n * h->n * sizeof(double2);
+  ck(cudaMemcpyAsync(staging, host, bytes, cudaMemcpyHostToDevice, h->stream), "upload");
+  sns::launch_full_to_half(staging, dst, herm, h->g, h->stream);
+}
+
+void download_full(sns_handle* h, const double2* src, double* host) {
+  double2* staging = h->wf(4);
+  const size_t bytes = (size_t)h->n * h->n * h->n * sizeof(double2);
+  sns::launch_half_to_full(src, staging, h->g, h->stream);
+  ck(cudaMemcpyAsync(host, staging, bytes, cudaMemcpyDeviceToHost, h->stream), "download");
+}
+
+// Physical velocity (energy, vmax^2) of the state: inverse z and y passes of u without the
+// phase shift, then the diagnostic x pass; results in h->red[0] (sum) and h->red[1] (max).
+void velocity_reductions(sns_handle* h) {
+  const sns::Ops* o = h->ops;
+  const sns::Geom& g = h->g;
+  const int tiles = h->nyq_clean ? h->tiles_data() : h->tiles_all();
+  o->zpass(h->u(), h->work, 3, +1, tiles, h->inv_size(), h->tw, g, h->stream);
+  o->ypass(h->work, 3, +1, tiles, h->tw, g, h->stream);
+  o->xpass_diag(h->work, h->u(), h->inv_size(), h->nyq_clean ? 1 : 0, h->partials, h->tw, g, h->stream);
+  const int rows = h->n * h->n;
+  sns::launch_reduce(h->partials, rows, 2, 0, h->red + 0, h->stream);
+  sns::launch_reduce(h->partials + 1, rows, 2, 1, h->red + 1, h->stream);
+}
+
+template <class F>
+int guarded(sns_handle* h, F&& f) {
+  if (h == nullptr) return SNS_ERR_INVALID;
+  try {
+    check_inject(h);
+    ck(cudaSetDevice(h->device), "cudaSetDevice");
+    f();
+    h->err.clear();
+    return SNS_OK;
+  } catch (const SnsError& e) {
+    h->err = e.msg;
+    return e.code;
+  } catch (const std::bad_alloc&) {
+    h->err = "host allocation failed";
+    return SNS_ERR_NOMEM;
+  } catch (const std::exception& e) {
+    h->err = e.what();
+    return SNS_ERR_INVALID;
+  }
+}
+
+void release(sns_handle* h) {
+  if (h == nullptr) return;
+  cudaSetDevice(h->device);
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  cudaFree(h->state);
+  cudaFree(h->work);
+  cudaFree(h->tw);
+  cudaFree(h->phase);
+  cudaFree(h->partials);
+  cudaFree(h->nyqsum);
+  cudaFree(h->red);
+  if (h->ev0) cudaEventDestroy(h->ev0);
+  if (h->ev1) cudaEventDestroy(h->ev1);
+  if (h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* sns_version(void) { return "sns_b200 0.1 (sm_100a, fp64 plain form)"; }
+
+size_t sns_bytes_required(int n, int precision) {
+  if (n <= 0 || precision != SNS_PRECISION_FP64) return 0;
+  return 18 * field_bytes(n) + partial_slots(n) * sizeof(double) + (size_t)(4 * n + 64) * sizeof(double2);
+}
+
+int sns_create(int n, double nu, int precision, int viscous_mode, uint64_t seed, double pert_amp, int pert_kmax,
+               sns_handle** out) {
+  g_create_error.clear();
+  if (out == nullptr) {
+    g_create_error = "null output pointer";
+    return SNS_ERR_INVALID;
+  }
+  *out = nullptr;
+  if (n <= 0) {
+    g_create_error = "grid size must be positive";
+    return SNS_ERR_INVALID;
+  }
+  if (!(nu >= 0.0) || !std::isfinite(nu)) {
+    g_create_error = "viscosity must be finite and non-negative (Reynolds number must be positive)";
+    return SNS_ERR_INVALID;
+  }
+  if (precision != SNS_PRECISION_FP64) {
+    g_create_error = "only the FP64 plain form is built";
+    return SNS_ERR_UNSUPPORTED;
+  }
+  if (viscous_mode != SNS_VISCOUS_EXPLICIT) {
+    g_create_error = "only the explicit viscous term (the reference's scheme) is built";
+    return SNS_ERR_UNSUPPORTED;
+  }
+  const sns::Ops* ops = sns::ops_for(n);
+  if (ops == nullptr) {
+    g_create_error = "grid size " + std::to_string(n) + " has no FFT plan (supported: 8 12 16 24 32 48 64 96 128 256 512)";
+    return SNS_ERR_UNSUPPORTED;
+  }
+  if (!(pert_amp >= 0.0) || (pert_amp > 0.0 && 2 * pert_kmax >= n)) {
+    g_create_error = "perturbation amplitude must be >= 0 and kmax below N/2";
+    return SNS_ERR_INVALID;
+  }
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    g_create_error = "no CUDA device visible";
+    return SNS_ERR_NO_DEVICE;
+  }
+  sns_handle* h = new (std::nothrow) sns_handle();
+  if (h == nullptr) {
+    g_create_error = "host allocation failed";
+    return SNS_ERR_NOMEM;
+  }
+  try {
+    ck(cudaGetDevice(&h->device), "cudaGetDevice");
+    h->n = n;
+    h->nu = nu;
+    h->precision = precision;
+    h->viscous_mode = viscous_mode;
+    h->ops = ops;
+    h->g = sns::Geom{n, n / 2, sns::pitch_for(n), (long long)n * n * sns::pitch_for(n)};
+    const size_t need = sns_bytes_required(n, precision);
+    size_t free_b = 0, total_b = 0;
+    ck(cudaMemGetInfo(&free_b, &total_b), "cudaMemGetInfo");
+    if (need > free_b) throw SnsError(SNS_ERR_NOMEM, "grid needs " + std::to_string(need) + " bytes, device has " +
+                                                         std::to_string(free_b) + " free");
+    ops->init();
+    ck(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    ck(cudaEventCreate(&h->ev0), "cudaEventCreate");
+    ck(cudaEventCreate(&h->ev1), "cudaEventCreate");
+    const size_t fb = field_bytes(n);
+    h->partial_count = partial_slots(n);
+    auto alloc = [&](void** p, size_t bytes) {
+      cudaError_t e = cudaMalloc(p, bytes);
+      if (e != cudaSuccess) {
+        cudaGetLastError();
+        throw SnsError(SNS_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+      }
+      h->bytes += bytes;
+    };
+    alloc((void**)&h->state, 6 * fb);
+    alloc((void**)&h->work, 12 * fb);
+    alloc((void**)&h->tw, (size_t)n * sizeof(double2));
+    alloc((void**)&h->phase, (size_t)(3 * n + 1) * sizeof(double2));
+    alloc((void**)&h->partials, h->partial_count * sizeof(double));
+    alloc((void**)&h->nyqsum, 16 * sizeof(double));
+    alloc((void**)&h->red, 16 * sizeof(double));
+    ck(cudaMemsetAsync(h->state, 0, 6 * fb, h->stream), "memset");
+    ck(cudaMemsetAsync(h->work, 0, 12 * fb, h->stream), "memset");
+    const auto tw = twiddle_table(n);
+    const auto ph = phase_table(n);
+    ck(cudaMemcpyAsync(h->tw, tw.data(), tw.size() * sizeof(double2), cudaMemcpyHostToDevice, h->stream), "tw");
+    ck(cudaMemcpyAsync(h->phase, ph.data(), ph.size() * sizeof(double2), cudaMemcpyHostToDevice, h->stream), "ph");
+    // Initial field: TGV at cell centres -> forward transform -> + perturbation -> project_truncate.
+    double* phys = reinterpret_cast<double*>(h->wf(6));
+    sns::launch_tgv_init(phys, h->g, h->stream);
+    ops->xpass_r2c(phys, h->u(), 2, h->tw, h->g, h->stream);  // w = 0: its spectrum stays zero
+    ops->ypass(h->u(), 2, -1, h->tiles_all(), h->tw, h->g, h->stream);
+    ops->zpass(h->u(), h->u(), 2, -1, h->tiles_all(), 1.0, h->tw, h->g, h->stream);
+    std::vector<long long> idx;
+    std::vector<double2> val;
+    perturbation_entries(n, seed, pert_amp, pert_kmax, h->g, idx, val);
+    if (!idx.empty()) {
+      long long* d_idx = reinterpret_cast<long long*>(h->wf(8));
+      double2* d_val = h->wf(9);
+      ck(cudaMemcpyAsync(d_idx, idx.data(), idx.size() * sizeof(long long), cudaMemcpyHostToDevice, h->stream), "p");
+      ck(cudaMemcpyAsync(d_val, val.data(), val.size() * sizeof(double2), cudaMemcpyHostToDevice, h->stream), "p");
+      sns::launch_add_sparse(h->u(), d_idx, d_val, (int)idx.size(), h->stream);
+      ck(cudaStreamSynchronize(h->stream), "perturbation");
+    }
+    sns::launch_project_truncate(h->u(), h->g, h->stream);
+    ck(cudaMemsetAsync(h->work, 0, 12 * fb, h->stream), "memset");
+    sync(h, "sns_create");
+  } catch (const SnsError& e) {
+    g_create_error = e.msg;
+    release(h);
+    return e.code;
+  } catch (const std::exception& e) {
+    g_create_error = e.what();
+    release(h);
+    return SNS_ERR_INVALID;
+  }
+  *out = h;
+  return SNS_OK;
+}
+
+int sns_destroy(sns_handle* h) {
+  if (h == nullptr) return SNS_ERR_INVALID;
+  release(h);
+  return SNS_OK;
+}
+
+const char* sns_last_error(const sns_handle* h) {
+  if (h == nullptr) return g_create_error.c_str();
+  return h->err.c_str();
+}
+
+int sns_grid_size(const sns_handle* h) { return h ? h->n : 0; }
+size_t sns_device_bytes(const sns_handle* h) { return h ? h->bytes : 0; }
+
+int sns_debug_fail_after(sns_handle* h, int k) {
+  if (h == nullptr) return SNS_ERR_INVALID;
+  h->fail_after = k > 0 ? k : 0;
+  return SNS_OK;
+}
+
+int sns_forward_r2c(sns_handle* h, const double* host_physical, double* host_spectral) {
+  return guarded(h, [&] {
+    if (!host_physical || !host_spectral) throw SnsError(SNS_ERR_INVALID, "null buffer");
+    const size_t np = (size_t)h->n * h->n * h->n;
+    double* phys = reinterpret_cast<double*>(h->wf(8));
+    ck(cudaMemcpyAsync(phys, host_physical, np * sizeof(double), cudaMemcpyHostToDevice, h->stream), "upload");
+    h->ops->xpass_r2c(phys, h->wf(0), 1, h->tw, h->g, h->stream);
+    h->ops->ypass(h->wf(0), 1, -1, h->tiles_all(), h->tw, h->g, h->stream);
+    h->ops->zpass(h->wf(0), h->wf(0), 1, -1, h->tiles_all(), 1.0, h->tw, h->g, h->stream);
+    download_full(h, h->wf(0), host_spectral);
+    sync(h, "sns_forward_r2c");
+  });
+}
+
+int sns_backward_c2r(sns_handle* h, const double* host_spectral, double* host_physical) {
+  return guarded(h, [&] {
+    if (!host_physical || !host_spectral) throw SnsError(SNS_ERR_INVALID, "null buffer");
+    const size_t np = (size_t)h->n * h->n * h->n;
+    upload_full(h, host_spectral, h->wf(0), 1);
+    h->ops->zpass(h->wf(0), h->wf(0), 1, +1, h->tiles_all(), h->inv_size(), h->tw, h->g, h->stream);
+    h->ops->ypass(h->wf(0), 1, +1, h->tiles_all(), h->tw, h->g, h->stream);
+    double* phys = reinterpret_cast<double*>(h->wf(8));
+    h->ops->xpass_c2r(h->wf(0), phys, 1, h->tw, h->g, h->stream);
+    ck(cudaMemcpyAsync(host_physical, phys, np * sizeof(double), cudaMemcpyDeviceToHost, h->stream), "download");
+    sync(h, "sns_backward_c2r");
+  });
+}
+
+int sns_set_state(sns_handle* h, const double* const uhat_full[3]) {
+  return guarded(h, [&] {
+    if (!uhat_full || !uhat_full[0] || !uhat_full[1] || !uhat_full[2]) throw SnsError(SNS_ERR_INVALID, "null buffer");
+    ck(cudaMemsetAsync(h->u(), 0, 3 * field_bytes(h->n), h->stream), "memset");
+    bool dirty = false;
+    for (int c = 0; c < 3; ++c) {
+      upload_full(h, uhat_full[c], h->u() + (long long)c * h->g.field, 0);
+      dirty = dirty || nyquist_plane_dirty(h->n, uhat_full[c]);
+      sync(h, "sns_set_state");
+    }
+    h->nyq_clean = !dirty;
+  });
+}
+
+int sns_get_state(sns_handle* h, double* const uhat_full[3]) {
+  return guarded(h, [&] {
+    if (!uhat_full || !uhat_full[0] || !uhat_full[1] || !uhat_full[2]) throw SnsError(SNS_ERR_INVALID, "null buffer");
+    for (int c = 0; c < 3; ++c) {
+      download_full(h, h->u() + (long long)c * h->g.field, uhat_full[c]);
+      sync(h, "sns_get_state");
+    }
+  });
+}
+
+int sns_rhs(sns_handle* h, const double* const uhat_full[3], double* const rhs_full[3]) {
+  return guarded(h, [&] {
+    if (!uhat_full || !rhs_full) throw SnsError(SNS_ERR_INVALID, "null buffer");
+    for (int c = 0; c < 3; ++c)
+      if (!uhat_full[c] || !rhs_full[c]) throw SnsError(SNS_ERR_INVALID, "null buffer");
+    // the RK scratch g doubles as the input state (g carries nothing between steps)
+    double2* uin = h->gb();
+    ck(cudaMemsetAsync(uin, 0, 3 * field_bytes(h->n), h->stream), "memset");
+    bool dirty = false;
+    for (int c = 0; c < 3; ++c) {
+      upload_full(h, uhat_full[c], uin + (long long)c * h->g.field, 0);
+      dirty = dirty || nyquist_plane_dirty(h->n, uhat_full[c]);
+      sync(h, "sns_rhs upload");
+    }
+    const bool saved = h->nyq_clean;
+    h->nyq_clean = !dirty;
+    run_stage(h, uin, nullptr, 0, 0.0, 1, h->work, nullptr);
+    h->nyq_clean = saved;
+    for (int c = 0; c < 3; ++c) {
+      download_full(h, h->wf(c), rhs_full[c]);
+      sync(h, "sns_rhs");
+    }
+  });
+}
+
+int sns_step(sns_handle* h, double dt, int nsteps) {
+  return guarded(h, [&] {
+    if (nsteps < 0 || !std::isfinite(dt)) throw SnsError(SNS_ERR_INVALID, "invalid dt or step count");
+    for (int s = 0; s < nsteps; ++s) step_once(h, dt);
+    sync(h, "sns_step");
+  });
+}
+
+int sns_time_steps(sns_handle* h, double dt, int nsteps, double* elapsed_ms) {
+  return guarded(h, [&] {
+    if (nsteps < 0 || !std::isfinite(dt) || !elapsed_ms) throw SnsError(SNS_ERR_INVALID, "invalid argument");
+    ck(cudaEventRecord(h->ev0, h->stream), "event");
+    for (int s = 0; s < nsteps; ++s) step_once(h, dt);
+    ck(cudaEventRecord(h->ev1, h->stream), "event");
+    sync(h, "sns_time_steps");
+    float ms = 0.f;
+    ck(cudaEventElapsedTime(&ms, h->ev0, h->ev1), "elapsed");
+    *elapsed_ms = ms;
+  });
+}
+
+int sns_profile_passes(sns_handle* h, double dt, int nsteps, double* pass_ms) {
+  return guarded(h, [&] {
+    if (nsteps <= 0 || !pass_ms) throw SnsError(SNS_ERR_INVALID, "invalid argument");
+    PassMarks pm;
+    pm.on = true;
+    for (int i = 0; i < 8; ++i) ck(cudaEventCreate(&pm.ev[i]), "event");
+    double acc[SNS_NUM_PASSES] = {0};
+    for (int s = 0; s < nsteps; ++s) {
+      for (int st = 0; st < 3; ++st) {
+        run_stage(h, h->u(), h->gb(), st, dt, 0, nullptr, nullptr, &pm);
+        sync(h, "sns_profile_passes");
+        for (int i = 0; i < SNS_NUM_PASSES; ++i) {
+          float ms = 0.f;
+          ck(cudaEventElapsedTime(&ms, pm.ev[i], pm.ev[i + 1]), "elapsed");
+          acc[i] += ms;
+        }
+      }
+    }
+    for (int i = 0; i < 8; ++i) cudaEventDestroy(pm.ev[i]);
+    for (int i = 0; i < SNS_NUM_PASSES; ++i) pass_ms[i] = acc[i] / (3.0 * nsteps);
+  });
+}
+
+int sns_max_velocity(sns_handle* h, double* out) {
+  return guarded(h, [&] {
+    if (!out) throw SnsError(SNS_ERR_INVALID, "null output");
+    velocity_reductions(h);
+    double r[2];
+    ck(cudaMemcpyAsync(r, h->red, 2 * sizeof(double), cudaMemcpyDeviceToHost, h->stream), "download");
+    sync(h, "sns_max_velocity");
+    *out = std::sqrt(r[1]);
+  });
+}
+
+int sns_diagnostics(sns_handle* h, double t, sns_diag* out) {
+  return guarded(h, [&] {
+    if (!out) throw SnsError(SNS_ERR_INVALID, "null output");
+    velocity_reductions(h);
+    const int nb = 1184;  // 8 CTAs per SM on 148 SMs
+    sns::launch_spectral_diag(h->u(), h->partials + 2 * (size_t)h->n * h->n, nb, h->g, h->stream);
+    sns::launch_reduce(h->partials + 2 * (size_t)h->n * h->n, nb, 2, 0, h->red + 2, h->stream);
+    sns::launch_reduce(h->partials + 2 * (size_t)h->n * h->n + 1, nb, 2, 1, h->red + 3, h->stream);
+    double r[4];
+    ck(cudaMemcpyAsync(r, h->red, 4 * sizeof(double), cudaMemcpyDeviceToHost, h->stream), "download");
+    sync(h, "sns_diagnostics");
+    const double n3 = (double)h->n * h->n * h->n;
+    out->t = t;
+    out->kinetic_energy = r[0] / n3;
+    out->enstrophy = 0.5 * r[2] / (n3 * n3);
+    out->dissipation = 2.0 * h->nu * out->enstrophy;
+    out->max_spectral_divergence = r[3];
+    out->max_velocity = std::sqrt(r[1]);
+  });
+}
+
+int sns_dump_velocity(sns_handle* h, double* const phys[3]) {
+  return guarded(h, [&] {
+    if (!phys || !phys[0] || !phys[1] || !phys[2]) throw SnsError(SNS_ERR_INVALID, "null buffer");
+    const size_t np = (size_t)h->n * h->n * h->n;
+    h->ops->zpass(h->u(), h->work, 3, +1, h->tiles_all(), h->inv_size(), h->tw, h->g, h->stream);
+    h->ops->ypass(h->work, 3, +1, h->tiles_all(), h->tw, h->g, h->stream);
+    double* real = reinterpret_cast<double*>(h->wf(4));
+    h->ops->xpass_c2r(h->work, real, 3, h->tw, h->g, h->stream);
+    for (int c = 0; c < 3; ++c)
+      ck(cudaMemcpyAsync(phys[c], real + c * np, np * sizeof(double), cudaMemcpyDeviceToHost, h->stream), "dl");
+    sync(h, "sns_dump_velocity");
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,216 @@
+// Shared-memory Stockham FFT engine for sm_100a (FP64 complex).
+//
+// A CTA transforms NSEQ independent sequences of length L that sit in shared memory.
+// Each radix-R stage is the Stockham autosort step (Stockham 1966; the GPU form of
+// Govindaraju et al., SC'08): butterfly j of a sequence reads elements j + r*L/R,
+// multiplies by W_{Ns*R}^{r*(j mod Ns)}, runs an R-point DFT in registers and writes
+// elements (j/Ns)*Ns*R + (j mod Ns) + r*Ns.  Output comes out in natural order, so no
+// bit reversal pass is needed.  Radices 2, 3, 4 and 8 are written out as register
+// butterflies; each length has a compile-time plan.
+//
+// Twiddles come from a per-CTA shared-memory table tw[t] = exp(-2*pi*i*t/L), t < L,
+// filled from a host-computed global table (no sin/cos on the device).
+//
+// Addressing is a policy: ColTile (y/z passes: element e of sequence s at e*NSEQ + s,
+// one 128-byte row of 8 sequences per element, conflict-free) or RowTile (x pass:
+// element e of sequence s at s*PITCH + e + e/8; the one-slot-per-8 padding keeps the
+// stride-R stores of the first stages free of bank conflicts).
+#pragma once
+
+#include <cuda_runtime.h>
+
+namespace sns {
+
+struct cplx_ops {
+  static __device__ __forceinline__ double2 add(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+  static __device__ __forceinline__ double2 sub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+};
+
+__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+// a * conj(b)
+__device__ __forceinline__ double2 cmulc(double2 a, double2 b) {
+  return make_double2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
+}
+__device__ __forceinline__ double2 cscale(double2 a, double s) { return make_double2(s * a.x, s * a.y); }
+__device__ __forceinline__ double2 cconj(double2 a) { return make_double2(a.x, -a.y); }
+// multiply by -i (DIR=-1) or +i (DIR=+1)
+template <int DIR>
+__device__ __forceinline__ double2 mul_dir_i(double2 a) {
+  if constexpr (DIR < 0) return make_double2(a.y, -a.x);
+  else return make_double2(-a.y, a.x);
+}
+
+// ------------------------------------------------------------------------------------
+// R-point DFTs in registers, sign DIR (-1 forward, +1 inverse), unnormalised.
+template <int DIR>
+__device__ __forceinline__ void dft2(double2* v) {
+  double2 a = v[0], b = v[1];
+  v[0] = cadd(a, b);
+  v[1] = csub(a, b);
+}
+
+template <int DIR>
+__device__ __forceinline__ void dft3(double2* v) {
+  constexpr double kS3 = 0.86602540378443864676372317075293618;  // sin(pi/3)
+  double2 a = v[0], b = v[1], c = v[2];
+  double2 t1 = cadd(b, c);
+  double2 t2 = make_double2(a.x - 0.5 * t1.x, a.y - 0.5 * t1.y);
+  double2 d = csub(b, c);
+  // DIR*i*sin(pi/3)*(b-c) with forward sign -1: y1 = t2 - i*s*d, y2 = t2 + i*s*d
+  double2 t3 = mul_dir_i<DIR>(make_double2(kS3 * d.x, kS3 * d.y));
+  v[0] = cadd(a, t1);
+  v[1] = cadd(t2, t3);
+  v[2] = csub(t2, t3);
+}
+
+template <int DIR>
+__device__ __forceinline__ void dft4(double2* v) {
+  double2 a = v[0], b = v[1], c = v[2], d = v[3];
+  double2 s0 = cadd(a, c), s1 = csub(a, c);
+  double2 s2 = cadd(b, d), s3 = mul_dir_i<DIR>(csub(b, d));
+  v[0] = cadd(s0, s2);
+  v[2] = csub(s0, s2);
+  v[1] = cadd(s1, s3);
+  v[3] = csub(s1, s3);
+}
+
+template <int DIR>
+__device__ __forceinline__ void dft8(double2* v) {
+  constexpr double kH = 0.70710678118654752440084436210484904;  // sqrt(2)/2
+  // radix-2 split into even/odd 4-point DFTs, then combine with W8^k
+  double2 e[4] = {v[0], v[2], v[4], v[6]};
+  double2 o[4] = {v[1], v[3], v[5], v[7]};
+  dft4<DIR>(e);
+  dft4<DIR>(o);
+  // W8^1 = (1 + DIR*i)/sqrt2 * ... : exp(DIR*i*pi/4) = kH*(1 + DIR*i)
+  double2 o1 = make_double2(kH * (o[1].x - DIR * o[1].y), kH * (o[1].y + DIR * o[1].x));
+  double2 o2 = mul_dir_i<DIR>(o[2]);
+  // W8^3 = exp(DIR*3i*pi/4) = kH*(-1 + DIR*i)
+  double2 o3 = make_double2(kH * (-o[3].x - DIR * o[3].y), kH * (-o[3].y + DIR * o[3].x));
+  v[0] = cadd(e[0], o[0]);
+  v[4] = csub(e[0], o[0]);
+  v[1] = cadd(e[1], o1);
+  v[5] = csub(e[1], o1);
+  v[2] = cadd(e[2], o2);
+  v[6] = csub(e[2], o2);
+  v[3] = cadd(e[3], o3);
+  v[7] = csub(e[3], o3);
+}
+
+template <int R, int DIR>
+__device__ __forceinline__ void dftR(double2* v) {
+  if constexpr (R == 2) dft2<DIR>(v);
+  else if constexpr (R == 3) dft3<DIR>(v);
+  else if constexpr (R == 4) dft4<DIR>(v);
+  else if constexpr (R == 8) dft8<DIR>(v);
+  else static_assert(R == 2, "unsupported radix");
+}
+
+// ------------------------------------------------------------------------------------
+// Plans: radices in application order.  Ns grows as the product of earlier radices.
+template <int... Rs>
+struct Radices {};
+
+template <int L>
+struct Plan;
+template <> struct Plan<2> { using type = Radices<2>; };
+template <> struct Plan<4> { using type = Radices<4>; };
+template <> struct Plan<6> { using type = Radices<3, 2>; };
+template <> struct Plan<8> { using type = Radices<8>; };
+template <> struct Plan<12> { using type = Radices<4, 3>; };
+template <> struct Plan<16> { using type = Radices<4, 4>; };
+template <> struct Plan<24> { using type = Radices<8, 3>; };
+template <> struct Plan<32> { using type = Radices<8, 4>; };
+template <> struct Plan<48> { using type = Radices<4, 4, 3>; };
+template <> struct Plan<64> { using type = Radices<8, 8>; };
+template <> struct Plan<96> { using type = Radices<8, 4, 3>; };
+template <> struct Plan<128> { using type = Radices<8, 4, 4>; };
+template <> struct Plan<256> { using type = Radices<8, 8, 4>; };
+template <> struct Plan<512> { using type = Radices<8, 8, 8>; };
+template <> struct Plan<1024> { using type = Radices<8, 8, 4, 4>; };
+
+// Addressing policies -----------------------------------------------------------------
+template <int NSEQ>
+struct ColTile {  // element e of sequence s -> e*NSEQ + s
+  static __device__ __forceinline__ int at(int s, int e) { return e * NSEQ + s; }
+  static constexpr bool kSeqFast = true;
+};
+
+template <int PITCH>
+struct RowTile {  // element e of sequence s -> s*PITCH + e + e/8
+  static __device__ __forceinline__ int at(int s, int e) { return s * PITCH + e + (e >> 3); }
+  static constexpr bool kSeqFast = false;
+};
+
+// Row pitch (in double2) of a padded RowTile sequence of length L.
+__host__ __device__ constexpr int row_pitch(int L) { return L + (L + 7) / 8; }
+
+// One Stockham stage for all NSEQ sequences, NT threads.
+template <int L, int DIR, int NSEQ, int NT, class Addr, int Ns, int R>
+__device__ __forceinline__ void fft_stage(double2* buf, const double2* tw, int tid) {
+  constexpr int kBf = L / R;               // butterflies per sequence
+  constexpr int kTot = NSEQ * kBf;          // butterflies in the tile
+  constexpr int kBpt = (kTot + NT - 1) / NT;
+  constexpr int kTwStep = L / (Ns * R);
+  double2 v[kBpt][R];
+#pragma unroll
+  for (int i = 0; i < kBpt; ++i) {
+    const int b = tid + i * NT;
+    if (kTot % NT == 0 || b < kTot) {
+      int s, j;
+      if constexpr (Addr::kSeqFast) { s = b % NSEQ; j = b / NSEQ; }
+      else { j = b % kBf; s = b / kBf; }
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[i][r] = buf[Addr::at(s, j + r * kBf)];
+      if constexpr (Ns > 1) {
+        const int k = j % Ns;
+#pragma unroll
+        for (int r = 1; r < R; ++r) {
+          double2 w = tw[r * k * kTwStep];
+          if constexpr (DIR > 0) w.y = -w.y;
+          v[i][r] = cmul(v[i][r], w);
+        }
+      }
+      dftR<R, DIR>(v[i]);
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < kBpt; ++i) {
+    const int b = tid + i * NT;
+    if (kTot % NT == 0 || b < kTot) {
+      int s, j;
+      if constexpr (Addr::kSeqFast) { s = b % NSEQ; j = b / NSEQ; }
+      else { j = b % kBf; s = b / kBf; }
+      const int k = j % Ns;
+      const int base = (j / Ns) * Ns * R + k;
+#pragma unroll
+      for (int r = 0; r < R; ++r) buf[Addr::at(s, base + r * Ns)] = v[i][r];
+    }
+  }
+  __syncthreads();
+}
+
+template <int L, int DIR, int NSEQ, int NT, class Addr, int Ns, int R, int... Rest>
+__device__ __forceinline__ void fft_stages(double2* buf, const double2* tw, int tid) {
+  fft_stage<L, DIR, NSEQ, NT, Addr, Ns, R>(buf, tw, tid);
+  if constexpr (sizeof...(Rest) > 0) fft_stages<L, DIR, NSEQ, NT, Addr, Ns * R, Rest...>(buf, tw, tid);
+}
+
+template <int L, int DIR, int NSEQ, int NT, class Addr, int... Rs>
+__device__ __forceinline__ void fft_run(double2* buf, const double2* tw, int tid, Radices<Rs...>) {
+  fft_stages<L, DIR, NSEQ, NT, Addr, 1, Rs...>(buf, tw, tid);
+}
+
+// Transform NSEQ sequences of length L in place.  Caller must __syncthreads() before
+// (data written) — the engine syncs after every stage, so the result is visible on return.
+template <int L, int DIR, int NSEQ, int NT, class Addr>
+__device__ __forceinline__ void smem_fft(double2* buf, const double2* tw, int tid) {
+  fft_run<L, DIR, NSEQ, NT, Addr>(buf, tw, tid, typename Plan<L>::type{});
+}
+
+}  // namespace sns

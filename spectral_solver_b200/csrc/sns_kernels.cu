@@ -1,0 +1,853 @@
+// Pass kernels of the B200 pseudo-spectral Taylor-Green step (FP64 plain form).
+//
+// One RK3 stage of the reference (ava_taylor_green_impl.hpp:847-977 compute_rhs plus the
+// stage update :994-1039) is five streaming passes over HBM:
+//   P1 zpass_inv_phase : inverse z transform of u_hat, both grids from one read
+//                        (the phase-shift kernel :866-873 fused in), 1/N^3 folded in
+//   P2 ypass (inverse) : 6 fields
+//   P3 xpass_products  : inverse x (c2r), the 6 products u_a*u_b on both grids,
+//                        forward x (r2c) of all 12 (product kernel :903-906 fused)
+//   P4 ypass (forward) : 12 fields
+//   P5 zpass (forward) + sweep : dealias combine, mask, -i k, viscous term, Leray
+//                        projection, low-storage RK3 update, projection of u
+//                        (accumulate :926-936, add_viscous_project :955-974,
+//                        RK update :994-1033, project_truncate :825-844)
+// Two real transforms share one complex FFT along x (z = u + i*u_shifted on the way in,
+// z = p0 + i*p_shifted on the way out), so every x transform is a full-length complex
+// FFT with no r2c post-twiddle.
+#include "sns_fft.cuh"
+#include "sns_kernels.cuh"
+
+#include <cstdio>
+
+namespace sns {
+
+constexpr int kT = 8;  // columns per y/z tile: 8 x 16 B = one 128-byte row segment
+
+__device__ __forceinline__ int signed_mode(int i, int n) { return i <= n / 2 ? i : i - n; }
+
+template <int N>
+__device__ __forceinline__ void load_twiddles(double2* sm_tw, const double2* tw, int tid, int nt) {
+  for (int t = tid; t < N; t += nt) sm_tw[t] = tw[t];
+}
+
+template <int N>
+constexpr int nt_yz() { return N < 32 ? 32 : (N > 256 ? 256 : N); }
+template <int N>
+constexpr int nt_x() { return N / 2 < 32 ? 32 : (N / 2 > 256 ? 256 : N / 2); }
+
+// ------------------------------------------------------------------------------------
+// P1: inverse z transform with the fused phase shift.
+// grid (ntiles, N [my], 3 [component]); tile = 8 columns x N rows (mz).
+template <int N>
+__global__ void __launch_bounds__(nt_yz<N>())
+k_zpass_inv_phase(const double2* __restrict__ u, double2* __restrict__ work, const double2* __restrict__ tw,
+                  const double2* __restrict__ phase, double scale, Geom g) {
+  constexpr int NT = nt_yz<N>();
+  extern __shared__ double2 smem[];
+  double2* s_tw = smem;
+  double2* tile = smem + N;
+  const int tid = threadIdx.x;
+  load_twiddles<N>(s_tw, tw, tid, NT);
+  const int mx0 = blockIdx.x * kT;
+  const int my = blockIdx.y;
+  const int c = blockIdx.z;
+  const double2* src = u + (long long)c * g.field;
+  double2* dst0 = work + (long long)(2 * c) * g.field;
+  double2* dst1 = work + (long long)(2 * c + 1) * g.field;
+  for (int e = tid; e < kT * N; e += NT) {
+    const int row = e / kT, col = e % kT;
+    tile[e] = cscale(src[((long long)row * N + my) * g.pitch + mx0 + col], scale);
+  }
+  __syncthreads();
+  smem_fft<N, +1, kT, NT, ColTile<kT>>(tile, s_tw, tid);
+  for (int e = tid; e < kT * N; e += NT) {
+    const int row = e / kT, col = e % kT;
+    dst0[((long long)row * N + my) * g.pitch + mx0 + col] = tile[e];
+  }
+  __syncthreads();
+  const int smy = signed_mode(my, N);
+  for (int e = tid; e < kT * N; e += NT) {
+    const int row = e / kT, col = e % kT;
+    // padding columns (> N/2) carry nothing; the Nyquist column mx = N/2 is transformed
+    // too (consumed only when the state's Nyquist plane has content off (N/2,0,0))
+    // Modes with 0 < mx < N/2 and index N/2 in exactly one of y, z: signed_mode gives +N/2
+    // to the mode and to its mirror, so phase(-m) = -conj(phase(m)) and the reference's
+    // shifted field is anti-Hermitian there; the real part it keeps of their inverse
+    // transform is zero.  (With N/2 in both the two shifts cancel.  All of these modes
+    // are zero in a masked state.)
+    const int mx = mx0 + col;
+    const bool anti = mx > 0 && mx < N / 2 && ((my == N / 2) != (row == N / 2));
+    if (mx <= N / 2 && !anti) {
+      const int msum = mx + smy + signed_mode(row, N);
+      const double2 v = cscale(src[((long long)row * N + my) * g.pitch + mx], scale);
+      tile[e] = cmul(v, phase[msum + 3 * N / 2]);
+    } else {
+      tile[e] = make_double2(0.0, 0.0);
+    }
+  }
+  __syncthreads();
+  smem_fft<N, +1, kT, NT, ColTile<kT>>(tile, s_tw, tid);
+  for (int e = tid; e < kT * N; e += NT) {
+    const int row = e / kT, col = e % kT;
+    dst1[((long long)row * N + my) * g.pitch + mx0 + col] = tile[e];
+  }
+}
+
+// y pass, in place.  grid (ntiles, N [z], nf).
+template <int N, int DIR>
+__global__ void __launch_bounds__(nt_yz<N>())
+k_ypass(double2* __restrict__ f, const double2* __restrict__ tw, Geom g) {
+  constexpr int NT = nt_yz<N>();
+  extern __shared__ double2 smem[];
+  double2* s_tw = smem;
+  double2* tile = smem + N;
+  const int tid = threadIdx.x;
+  load_twiddles<N>(s_tw, tw, tid, NT);
+  const int mx0 = blockIdx.x * kT;
+  const int z = blockIdx.y;
+  double2* fld = f + (long long)blockIdx.z * g.field;
+  for (int e = tid; e < kT * N; e += NT) {
+    const int row = e / kT, col = e % kT;
+    tile[e] = fld[((long long)z * N + row) * g.pitch + mx0 + col];
+  }
+  __syncthreads();
+  smem_fft<N, DIR, kT, NT, ColTile<kT>>(tile, s_tw, tid);
+  for (int e = tid; e < kT * N; e += NT) {
+    const int row = e / kT, col = e % kT;
+    fld[((long long)z * N + row) * g.pitch + mx0 + col] = tile[e];
+  }
+}
+
+// z pass, src -> dst (may alias), optional scale on load.  grid (ntiles, N [y], nf).
+template <int N, int DIR>
+__global__ void __launch_bounds__(nt_yz<N>())
+k_zpass(const double2* src, double2* dst, double scale, const double2* __restrict__ tw, Geom g) {
+  constexpr int NT = nt_yz<N>();
+  extern __shared__ double2 smem[];
+  double2* s_tw = smem;
+  double2* tile = smem + N;
+  const int tid = threadIdx.x;
+  load_twiddles<N>(s_tw, tw, tid, NT);
+  const int mx0 = blockIdx.x * kT;
+  const int y = blockIdx.y;
+  const double2* fin = src + (long long)blockIdx.z * g.field;
+  double2* fout = dst + (long long)blockIdx.z * g.field;
+  for (int e = tid; e < kT * N; e += NT) {
+    const int row = e / kT, col = e % kT;
+    tile[e] = cscale(fin[((long long)row * N + y) * g.pitch + mx0 + col], scale);
+  }
+  __syncthreads();
+  smem_fft<N, DIR, kT, NT, ColTile<kT>>(tile, s_tw, tid);
+  for (int e = tid; e < kT * N; e += NT) {
+    const int row = e / kT, col = e % kT;
+    fout[((long long)row * N + y) * g.pitch + mx0 + col] = tile[e];
+  }
+}
+
+// ------------------------------------------------------------------------------------
+// Packing two Hermitian half spectra A, B (k in [0, N/2]) into Z = A + iB over k in [0, N).
+// At k = 0 and k = N/2 only the real parts enter: that is the Hermitian part of the
+// (y,z)-transformed mx = 0 and mx = N/2 planes, i.e. Re(IDFT) of the reference.
+__device__ __forceinline__ void pack_pair(double2 A, double2 B, int k, int nh, int n, double2* seq_at_k,
+                                          double2* seq_at_mirror) {
+  if (k == 0 || k == nh) {
+    *seq_at_k = make_double2(A.x, B.x);
+  } else {
+    *seq_at_k = make_double2(A.x - B.y, A.y + B.x);
+    *seq_at_mirror = make_double2(A.x + B.y, B.x - A.y);
+  }
+}
+
+// Unpack Z = FFT(a + i b) into the half spectra of a and b at k.
+__device__ __forceinline__ void unpack_pair(double2 Zk, double2 Zm, double2* A, double2* B) {
+  *A = make_double2(0.5 * (Zk.x + Zm.x), 0.5 * (Zk.y - Zm.y));
+  *B = make_double2(0.5 * (Zk.y + Zm.y), -0.5 * (Zk.x - Zm.x));
+}
+
+template <int NT>
+__device__ __forceinline__ void block_sum_max(double& s, double& m, double* red) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    s += __shfl_xor_sync(0xffffffffu, s, o);
+    m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  }
+  constexpr int NW = NT / 32;
+  const int w = threadIdx.x / 32, l = threadIdx.x % 32;
+  __syncthreads();
+  if (l == 0) { red[w] = s; red[NW + w] = m; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double ss = 0.0, mm = 0.0;
+    for (int i = 0; i < NW; ++i) { ss += red[i]; mm = fmax(mm, red[NW + i]); }
+    s = ss;
+    m = mm;
+  }
+}
+
+// P3: fused inverse x / products / forward x.  One row (y, z) per CTA.
+// Input work fields 0..5 = (U_0, V_0, U_1, V_1, U_2, V_2) [V = shifted grid] after the
+// y and z inverse passes; output work fields 2p, 2p+1 = (P0_p, Ps_p) for the pairs
+// p = 00, 01, 02, 11, 12, 22, columns 0..N/2 (column N/2: per-row Nyquist value).
+template <int N>
+__global__ void __launch_bounds__(nt_x<N>())
+k_xpass_products(double2* __restrict__ work, const double2* __restrict__ unyq, const double2* __restrict__ phase,
+                 double scale, int nyq_scalar, double* __restrict__ partials, const double2* __restrict__ tw,
+                 Geom g) {
+  constexpr int NT = nt_x<N>();
+  constexpr int NH = N / 2;
+  constexpr int RP = row_pitch(N);
+  extern __shared__ double2 smem[];
+  double2* s_tw = smem;
+  double2* seq = smem + N;  // 6 sequences of pitch RP
+  __shared__ double red[2 * (NT / 32)];
+  const int tid = threadIdx.x;
+  load_twiddles<N>(s_tw, tw, tid, NT);
+  const long long row = blockIdx.x;
+  const long long rbase = row * g.pitch;
+  // pack Z_c = U_c + i V_c
+  for (int e = tid; e < 3 * (NH + 1); e += NT) {
+    const int c = e / (NH + 1), k = e % (NH + 1);
+    double2 A, B;
+    if (k == NH && nyq_scalar) {
+      // masked state: the mx = N/2 plane holds only (N/2,0,0); after the y/z inverse
+      // transforms it is the constant c_N (and phase(N/2,0,0)*c_N on the shifted grid).
+      const double2 cn = cscale(unyq[(long long)c * g.field + NH], scale);
+      A = cn;
+      B = cmul(cn, phase[NH + 3 * N / 2]);
+    } else {
+      A = work[(long long)(2 * c) * g.field + rbase + k];
+      B = work[(long long)(2 * c + 1) * g.field + rbase + k];
+    }
+    double2* sq = seq + c * RP;
+    double2 zk, zm;
+    pack_pair(A, B, k, NH, N, &zk, &zm);
+    sq[k + (k >> 3)] = zk;
+    if (k != 0 && k != NH) sq[(N - k) + ((N - k) >> 3)] = zm;
+  }
+  __syncthreads();
+  smem_fft<N, +1, 3, NT, RowTile<RP>>(seq, s_tw, tid);
+  double esum = 0.0, vmax2 = 0.0;
+  for (int x = tid; x < N; x += NT) {
+    const int p = x + (x >> 3);
+    const double2 z0 = seq[p], z1 = seq[RP + p], z2 = seq[2 * RP + p];
+    const double s2 = z0.x * z0.x + z1.x * z1.x + z2.x * z2.x;
+    esum += 0.5 * s2;
+    vmax2 = fmax(vmax2, s2);
+    seq[0 * RP + p] = make_double2(z0.x * z0.x, z0.y * z0.y);
+    seq[1 * RP + p] = make_double2(z0.x * z1.x, z0.y * z1.y);
+    seq[2 * RP + p] = make_double2(z0.x * z2.x, z0.y * z2.y);
+    seq[3 * RP + p] = make_double2(z1.x * z1.x, z1.y * z1.y);
+    seq[4 * RP + p] = make_double2(z1.x * z2.x, z1.y * z2.y);
+    seq[5 * RP + p] = make_double2(z2.x * z2.x, z2.y * z2.y);
+  }
+  if (partials != nullptr) {
+    block_sum_max<NT>(esum, vmax2, red);
+    if (tid == 0) {
+      partials[2 * row] = esum;
+      partials[2 * row + 1] = vmax2;
+    }
+  }
+  __syncthreads();
+  smem_fft<N, -1, 6, NT, RowTile<RP>>(seq, s_tw, tid);
+  for (int e = tid; e < 6 * (NH + 1); e += NT) {
+    const int pr = e / (NH + 1), k = e % (NH + 1);
+    const int km = (N - k) % N;
+    const double2 Zk = seq[pr * RP + k + (k >> 3)];
+    const double2 Zm = seq[pr * RP + km + (km >> 3)];
+    double2 A, B;
+    unpack_pair(Zk, Zm, &A, &B);
+    work[(long long)(2 * pr) * g.field + rbase + k] = A;
+    work[(long long)(2 * pr + 1) * g.field + rbase + k] = B;
+  }
+}
+
+// Nyquist-plane sums: column N/2 of each of the 12 product fields summed over all rows
+// (the (N/2,0,0) output of the y/z forward transforms is the plain sum of the plane).
+// grid 12, fixed summation order.
+__global__ void __launch_bounds__(256) k_nyq_reduce(const double2* __restrict__ work, double* __restrict__ sums,
+                                                    Geom g) {
+  __shared__ double red[256];
+  const double2* f = work + (long long)blockIdx.x * g.field + g.nh;
+  const long long rows = (long long)g.n * g.n;
+  double s = 0.0;
+  for (long long r = threadIdx.x; r < rows; r += 256) s += f[r * g.pitch].x;
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) sums[blockIdx.x] = red[0];
+}
+
+// ------------------------------------------------------------------------------------
+// P5 sweep: per mode, the reference's accumulate (:926-936), add_viscous_project
+// (:955-974), RK stage update (:994-1033) and project_truncate (:825-844).
+struct ModeIn {
+  double2 p0[6];
+  double2 ps[6];
+};
+
+__device__ __forceinline__ double2 minus_i_k(double2 a, int k) {
+  const double rk = (double)k;
+  return make_double2(rk * a.y, -rk * a.x);
+}
+
+__device__ __forceinline__ void sweep_mode(const ModeIn& in, int ix, int iy, int iz, int n, double2 phase,
+                                           double2 uu[3], double2 gg[3], bool load_g, double2 rr[3],
+                                           const SweepArgs& a) {
+  const int m2 = ix * ix + iy * iy + iz * iz;
+  const bool keep = 4LL * m2 <= (long long)n * n;
+  const int kv[3] = {ix, iy, iz};
+  double2 r[3] = {make_double2(0, 0), make_double2(0, 0), make_double2(0, 0)};
+  const int pa[6] = {0, 0, 0, 1, 1, 2};
+  const int pb[6] = {0, 1, 2, 1, 2, 2};
+#pragma unroll
+  for (int p = 0; p < 6; ++p) {
+    double2 value;
+    if (a.dealias) value = cscale(cadd(in.p0[p], cmulc(in.ps[p], phase)), 0.5);
+    else value = in.p0[p];
+    if (!keep) value = make_double2(0.0, 0.0);
+    r[pa[p]] = cadd(r[pa[p]], minus_i_k(value, kv[pb[p]]));
+    if (pa[p] != pb[p]) r[pb[p]] = cadd(r[pb[p]], minus_i_k(value, kv[pa[p]]));
+  }
+  const double k2 = (double)m2;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) r[c] = csub(r[c], cscale(uu[c], a.nu * k2));
+  if (k2 > 0.0 && keep) {
+    const double2 dot = cadd(cadd(cscale(r[0], (double)ix), cscale(r[1], (double)iy)), cscale(r[2], (double)iz));
+    const double2 factor = cscale(dot, 1.0 / k2);
+    r[0] = csub(r[0], cscale(factor, (double)ix));
+    r[1] = csub(r[1], cscale(factor, (double)iy));
+    r[2] = csub(r[2], cscale(factor, (double)iz));
+  } else {
+    r[0] = r[1] = r[2] = make_double2(0.0, 0.0);
+  }
+  if (a.mode == 1) {
+    rr[0] = r[0];
+    rr[1] = r[1];
+    rr[2] = r[2];
+    return;
+  }
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    gg[c] = load_g ? cadd(cscale(gg[c], a.ga), r[c]) : r[c];
+    uu[c] = cadd(uu[c], cscale(gg[c], a.ub));
+  }
+  if (k2 > 0.0 && keep) {
+    const double2 dot = cadd(cadd(cscale(uu[0], (double)ix), cscale(uu[1], (double)iy)), cscale(uu[2], (double)iz));
+    const double2 factor = cscale(dot, 1.0 / k2);
+    uu[0] = csub(uu[0], cscale(factor, (double)ix));
+    uu[1] = csub(uu[1], cscale(factor, (double)iy));
+    uu[2] = csub(uu[2], cscale(factor, (double)iz));
+  } else {
+    uu[0] = uu[1] = uu[2] = make_double2(0.0, 0.0);
+  }
+}
+
+template <int N>
+__global__ void __launch_bounds__(256)
+k_sweep(const double2* __restrict__ work, double2* __restrict__ u, double2* __restrict__ gbuf,
+        double2* __restrict__ rhs, const double* __restrict__ nyqsum, const double2* __restrict__ phase,
+        SweepArgs a, Geom g) {
+  constexpr int NH = N / 2;
+  const long long e = (long long)blockIdx.x * 256 + threadIdx.x;
+  const long long total = (long long)N * N * NH;
+  const bool load_g = a.stage > 0;
+  if (e < total) {
+    const long long row = e / NH;
+    const int mx = (int)(e % NH);
+    const int my = signed_mode((int)(row % N), N);
+    const int mz = signed_mode((int)(row / N), N);
+    const long long idx = row * g.pitch + mx;
+    ModeIn in;
+#pragma unroll
+    for (int p = 0; p < 6; ++p) {
+      in.p0[p] = work[(long long)(2 * p) * g.field + idx];
+      in.ps[p] = work[(long long)(2 * p + 1) * g.field + idx];
+    }
+    double2 uu[3], gg[3], rr[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      uu[c] = u[(long long)c * g.field + idx];
+      gg[c] = load_g ? gbuf[(long long)c * g.field + idx] : make_double2(0, 0);
+    }
+    sweep_mode(in, mx, my, mz, N, phase[mx + my + mz + 3 * N / 2], uu, gg, load_g, rr, a);
+    if (a.mode == 1) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) rhs[(long long)c * g.field + idx] = rr[c];
+    } else {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        u[(long long)c * g.field + idx] = uu[c];
+        gbuf[(long long)c * g.field + idx] = gg[c];
+      }
+    }
+    // The plane mx = N/2 is outside the sphere except at (N/2,0,0): the reference's
+    // masked RHS, g and projected u are zero there.  Row 0 is written below.
+    if (mx == 0 && row != 0) {
+      const long long inq = row * g.pitch + NH;
+      const double2 zero = make_double2(0.0, 0.0);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        if (a.mode == 1) {
+          rhs[(long long)c * g.field + inq] = zero;
+        } else {
+          u[(long long)c * g.field + inq] = zero;
+          gbuf[(long long)c * g.field + inq] = zero;
+        }
+      }
+    }
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    // the self-conjugate Nyquist mode (N/2, 0, 0), column nh of row (0, 0)
+    ModeIn in;
+#pragma unroll
+    for (int p = 0; p < 6; ++p) {
+      in.p0[p] = make_double2(nyqsum[2 * p], 0.0);
+      in.ps[p] = make_double2(nyqsum[2 * p + 1], 0.0);
+    }
+    const long long idx = NH;
+    double2 uu[3], gg[3], rr[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      uu[c] = u[(long long)c * g.field + idx];
+      gg[c] = load_g ? gbuf[(long long)c * g.field + idx] : make_double2(0, 0);
+    }
+    sweep_mode(in, NH, 0, 0, N, phase[NH + 3 * N / 2], uu, gg, load_g, rr, a);
+    if (a.mode == 1) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) rhs[(long long)c * g.field + idx] = rr[c];
+    } else {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        u[(long long)c * g.field + idx] = uu[c];
+        gbuf[(long long)c * g.field + idx] = gg[c];
+      }
+    }
+  }
+}
+
+// ------------------------------------------------------------------------------------
+// Generic x transforms (FFT-backend contract and initialisation).  Two rows of one field
+// share a complex FFT.  grid (N*N/2, nf).
+template <int N>
+__global__ void __launch_bounds__(nt_x<N>())
+k_xpass_r2c(const double* __restrict__ in, double2* __restrict__ out, const double2* __restrict__ tw, Geom g) {
+  constexpr int NT = nt_x<N>();
+  constexpr int NH = N / 2;
+  constexpr int RP = row_pitch(N);
+  extern __shared__ double2 smem[];
+  double2* s_tw = smem;
+  double2* seq = smem + N;
+  const int tid = threadIdx.x;
+  load_twiddles<N>(s_tw, tw, tid, NT);
+  const long long r0 = 2LL * blockIdx.x;
+  const double* fin = in + (long long)blockIdx.y * N * N * N;
+  double2* fout = out + (long long)blockIdx.y * g.field;
+  for (int x = tid; x < N; x += NT) seq[x + (x >> 3)] = make_double2(fin[r0 * N + x], fin[(r0 + 1) * N + x]);
+  __syncthreads();
+  smem_fft<N, -1, 1, NT, RowTile<RP>>(seq, s_tw, tid);
+  for (int k = tid; k <= NH; k += NT) {
+    const int km = (N - k) % N;
+    double2 A, B;
+    unpack_pair(seq[k + (k >> 3)], seq[km + (km >> 3)], &A, &B);
+    fout[r0 * g.pitch + k] = A;
+    fout[(r0 + 1) * g.pitch + k] = B;
+  }
+}
+
+template <int N>
+__global__ void __launch_bounds__(nt_x<N>())
+k_xpass_c2r(const double2* __restrict__ in, double* __restrict__ out, const double2* __restrict__ tw, Geom g) {
+  constexpr int NT = nt_x<N>();
+  constexpr int NH = N / 2;
+  constexpr int RP = row_pitch(N);
+  extern __shared__ double2 smem[];
+  double2* s_tw = smem;
+  double2* seq = smem + N;
+  const int tid = threadIdx.x;
+  load_twiddles<N>(s_tw, tw, tid, NT);
+  const long long r0 = 2LL * blockIdx.x;
+  const double2* fin = in + (long long)blockIdx.y * g.field;
+  double* fout = out + (long long)blockIdx.y * N * N * N;
+  for (int k = tid; k <= NH; k += NT) {
+    double2 zk, zm;
+    pack_pair(fin[r0 * g.pitch + k], fin[(r0 + 1) * g.pitch + k], k, NH, N, &zk, &zm);
+    seq[k + (k >> 3)] = zk;
+    if (k != 0 && k != NH) seq[(N - k) + ((N - k) >> 3)] = zm;
+  }
+  __syncthreads();
+  smem_fft<N, +1, 1, NT, RowTile<RP>>(seq, s_tw, tid);
+  for (int x = tid; x < N; x += NT) {
+    const double2 v = seq[x + (x >> 3)];
+    fout[r0 * N + x] = v.x;
+    fout[(r0 + 1) * N + x] = v.y;
+  }
+}
+
+// Energy / vmax partials of the physical velocity (work fields 0,1,2 after the inverse
+// z and y passes of u_hat without phase shift).  One row per CTA.
+template <int N>
+__global__ void __launch_bounds__(nt_x<N>())
+k_xpass_diag(const double2* __restrict__ work, const double2* __restrict__ unyq, double scale, int nyq_scalar,
+             double* __restrict__ partials, const double2* __restrict__ tw, Geom g) {
+  constexpr int NT = nt_x<N>();
+  constexpr int NH = N / 2;
+  constexpr int RP = row_pitch(N);
+  extern __shared__ double2 smem[];
+  double2* s_tw = smem;
+  double2* seq = smem + N;  // 2 sequences: u0 + i u1, u2
+  __shared__ double red[2 * (NT / 32)];
+  const int tid = threadIdx.x;
+  load_twiddles<N>(s_tw, tw, tid, NT);
+  const long long row = blockIdx.x;
+  const long long rbase = row * g.pitch;
+  for (int k = tid; k <= NH; k += NT) {
+    double2 U[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      if (k == NH && nyq_scalar) U[c] = cscale(unyq[(long long)c * g.field + NH], scale);
+      else U[c] = work[(long long)c * g.field + rbase + k];
+    }
+    double2 zk, zm;
+    pack_pair(U[0], U[1], k, NH, N, &zk, &zm);
+    seq[k + (k >> 3)] = zk;
+    if (k != 0 && k != NH) seq[(N - k) + ((N - k) >> 3)] = zm;
+    pack_pair(U[2], make_double2(0.0, 0.0), k, NH, N, &zk, &zm);
+    seq[RP + k + (k >> 3)] = zk;
+    if (k != 0 && k != NH) seq[RP + (N - k) + ((N - k) >> 3)] = zm;
+  }
+  __syncthreads();
+  smem_fft<N, +1, 2, NT, RowTile<RP>>(seq, s_tw, tid);
+  double esum = 0.0, vmax2 = 0.0;
+  for (int x = tid; x < N; x += NT) {
+    const int p = x + (x >> 3);
+    const double2 a = seq[p], b = seq[RP + p];
+    const double s2 = a.x * a.x + a.y * a.y + b.x * b.x;
+    esum += 0.5 * s2;
+    vmax2 = fmax(vmax2, s2);
+  }
+  block_sum_max<NT>(esum, vmax2, red);
+  if (tid == 0) {
+    partials[2 * row] = esum;
+    partials[2 * row + 1] = vmax2;
+  }
+}
+
+// ------------------------------------------------------------------------------------
+// Size-independent kernels.
+
+// Taylor-Green field at cell centres (ava_taylor_green_impl.hpp:805-812), x fastest.
+__global__ void k_tgv_init(double* __restrict__ phys, int n) {
+  const long long np = (long long)n * n * n;
+  const long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (id >= np) return;
+  constexpr double kPi = 3.141592653589793238462643383279502884;
+  const int ix = (int)(id % n), iy = (int)((id / n) % n), iz = (int)(id / ((long long)n * n));
+  const double x = ((double)ix + 0.5) * 2.0 * kPi / (double)n;
+  const double y = ((double)iy + 0.5) * 2.0 * kPi / (double)n;
+  const double z = ((double)iz + 0.5) * 2.0 * kPi / (double)n;
+  phys[id] = sin(x) * cos(y) * cos(z);
+  phys[np + id] = -cos(x) * sin(y) * cos(z);
+  phys[2 * np + id] = 0.0;
+}
+
+// project_truncate over every stored mode, Nyquist column included (:825-844).
+__global__ void k_project_truncate(double2* __restrict__ u, Geom g) {
+  const long long total = (long long)g.n * g.n * (g.nh + 1);
+  const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= total) return;
+  const long long row = e / (g.nh + 1);
+  const int ix = (int)(e % (g.nh + 1));
+  const int iy = signed_mode((int)(row % g.n), g.n);
+  const int iz = signed_mode((int)(row / g.n), g.n);
+  const long long idx = row * g.pitch + ix;
+  const int m2 = ix * ix + iy * iy + iz * iz;
+  const bool keep = 4LL * m2 <= (long long)g.n * g.n;
+  const double k2 = (double)m2;
+  double2 ux = u[idx], uy = u[g.field + idx], uz = u[2 * g.field + idx];
+  if (k2 > 0.0 && keep) {
+    const double2 dot = cadd(cadd(cscale(ux, (double)ix), cscale(uy, (double)iy)), cscale(uz, (double)iz));
+    const double2 factor = cscale(dot, 1.0 / k2);
+    ux = csub(ux, cscale(factor, (double)ix));
+    uy = csub(uy, cscale(factor, (double)iy));
+    uz = csub(uz, cscale(factor, (double)iz));
+  } else {
+    ux = uy = uz = make_double2(0.0, 0.0);
+  }
+  u[idx] = ux;
+  u[g.field + idx] = uy;
+  u[2 * g.field + idx] = uz;
+}
+
+__global__ void k_add_sparse(double2* __restrict__ u, const long long* __restrict__ idx,
+                             const double2* __restrict__ val, int count) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  const long long at = idx[i];
+  u[at] = cadd(u[at], val[i]);
+}
+
+// half -> reference full layout (mx < 0 from the conjugate mirror).
+__global__ void k_half_to_full(const double2* __restrict__ half, double2* __restrict__ full, Geom g) {
+  const long long n = g.n;
+  const long long total = n * n * n;
+  const long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (id >= total) return;
+  const int x = (int)(id % n);
+  const long long y = (id / n) % n, z = id / (n * n);
+  if (x <= g.nh) {
+    full[id] = half[(z * n + y) * g.pitch + x];
+  } else {
+    const long long ym = (n - y) % n, zm = (n - z) % n;
+    full[id] = cconj(half[(zm * n + ym) * g.pitch + (n - x)]);
+  }
+}
+
+// reference full layout -> half; with hermitian_part the Hermitian part
+// (c_m + conj(c_-m))/2 is stored, so a c2r of the result equals Re(IDFT(c)).
+__global__ void k_full_to_half(const double2* __restrict__ full, double2* __restrict__ half, int hermitian_part,
+                               Geom g) {
+  const long long n = g.n;
+  const long long total = n * n * (g.nh + 1);
+  const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= total) return;
+  const long long row = e / (g.nh + 1);
+  const int x = (int)(e % (g.nh + 1));
+  const long long y = row % n, z = row / n;
+  double2 v = full[(z * n + y) * n + x];
+  if (hermitian_part) {
+    const long long ym = (n - y) % n, zm = (n - z) % n, xm = (n - x) % n;
+    const double2 w = full[(zm * n + ym) * n + xm];
+    v = make_double2(0.5 * (v.x + w.x), 0.5 * (v.y - w.y));
+  }
+  half[row * g.pitch + x] = v;
+}
+
+// Parseval enstrophy and max spectral divergence of the (masked) state.
+// Enstrophy = 0.5/N^6 * sum_m |H(omega_hat)_m|^2 over the full spectrum, with
+// omega_hat = i k x u_hat as the reference forms it (:1147-1157).  Planes mx = 0 and
+// mx = N/2 are their own x-mirror: weight 1 and the in-plane Hermitian part; other
+// columns stand for themselves and their conjugate mirror: weight 2.
+__device__ __forceinline__ void omega_hat(const double2* u, long long field, long long idx, int ix, int iy, int iz,
+                                          double2 w[3]) {
+  const double2 u0 = u[idx], u1 = u[field + idx], u2 = u[2 * field + idx];
+  const double rx = ix, ry = iy, rz = iz;
+  w[0] = make_double2(-(ry * u2.y - rz * u1.y), ry * u2.x - rz * u1.x);
+  w[1] = make_double2(-(rz * u0.y - rx * u2.y), rz * u0.x - rx * u2.x);
+  w[2] = make_double2(-(rx * u1.y - ry * u0.y), rx * u1.x - ry * u0.x);
+}
+
+__global__ void __launch_bounds__(256) k_spectral_diag(const double2* __restrict__ u, double* __restrict__ partials,
+                                                       Geom g) {
+  __shared__ double red_s[256];
+  __shared__ double red_m[256];
+  const long long total = (long long)g.n * g.n * (g.nh + 1);
+  double s = 0.0, m = 0.0;
+  for (long long e = (long long)blockIdx.x * 256 + threadIdx.x; e < total; e += (long long)gridDim.x * 256) {
+    const long long row = e / (g.nh + 1);
+    const int ix = (int)(e % (g.nh + 1));
+    const int yi = (int)(row % g.n), zi = (int)(row / g.n);
+    const int iy = signed_mode(yi, g.n), iz = signed_mode(zi, g.n);
+    const long long idx = row * g.pitch + ix;
+    double2 w[3];
+    omega_hat(u, g.field, idx, ix, iy, iz, w);
+    double contrib;
+    if (ix == 0 || ix == g.nh) {
+      const int ym = (g.n - yi) % g.n, zm = (g.n - zi) % g.n;
+      const long long idm = ((long long)zm * g.n + ym) * g.pitch + ix;
+      double2 wm[3];
+      omega_hat(u, g.field, idm, ix, signed_mode(ym, g.n), signed_mode(zm, g.n), wm);
+      contrib = 0.0;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const double hx = 0.5 * (w[c].x + wm[c].x), hy = 0.5 * (w[c].y - wm[c].y);
+        contrib += hx * hx + hy * hy;
+      }
+    } else if (yi == g.n / 2 || zi == g.n / 2) {
+      // mirror -m is not stored; its value is conj(u_m) but its wavenumber keeps +N/2 on the
+      // Nyquist axis, so omega_hat(-m) is not conj(omega_hat(m)): form H explicitly.
+      const int my2 = yi == g.n / 2 ? iy : -iy, mz2 = zi == g.n / 2 ? iz : -iz;
+      const double2 u0 = u[idx], u1 = u[g.field + idx], u2 = u[2 * g.field + idx];
+      const double2 c0 = cconj(u0), c1 = cconj(u1), c2 = cconj(u2);
+      const double rx = -ix, ry = my2, rz = mz2;
+      double2 wm[3];
+      wm[0] = make_double2(-(ry * c2.y - rz * c1.y), ry * c2.x - rz * c1.x);
+      wm[1] = make_double2(-(rz * c0.y - rx * c2.y), rz * c0.x - rx * c2.x);
+      wm[2] = make_double2(-(rx * c1.y - ry * c0.y), rx * c1.x - ry * c0.x);
+      contrib = 0.0;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const double hx = 0.5 * (w[c].x + wm[c].x), hy = 0.5 * (w[c].y - wm[c].y);
+        contrib += 2.0 * (hx * hx + hy * hy);
+      }
+      const double2 dm = cadd(cadd(cscale(c0, rx), cscale(c1, ry)), cscale(c2, rz));
+      m = fmax(m, sqrt(dm.x * dm.x + dm.y * dm.y));
+    } else {
+      contrib = 0.0;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) contrib += 2.0 * (w[c].x * w[c].x + w[c].y * w[c].y);
+    }
+    s += contrib;
+    const double2 u0 = u[idx], u1 = u[g.field + idx], u2 = u[2 * g.field + idx];
+    const double2 div = cadd(cadd(cscale(u0, (double)ix), cscale(u1, (double)iy)), cscale(u2, (double)iz));
+    m = fmax(m, sqrt(div.x * div.x + div.y * div.y));
+  }
+  red_s[threadIdx.x] = s;
+  red_m[threadIdx.x] = m;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if (threadIdx.x < o) {
+      red_s[threadIdx.x] += red_s[threadIdx.x + o];
+      red_m[threadIdx.x] = fmax(red_m[threadIdx.x], red_m[threadIdx.x + o]);
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    partials[2 * blockIdx.x] = red_s[0];
+    partials[2 * blockIdx.x + 1] = red_m[0];
+  }
+}
+
+// Fixed-order reduction of `count` partials at stride `stride` (one CTA).
+__global__ void __launch_bounds__(256) k_reduce(const double* __restrict__ partials, int count, int stride,
+                                                int op_max, double* __restrict__ out) {
+  __shared__ double red[256];
+  double s = 0.0;
+  for (int i = threadIdx.x; i < count; i += 256) {
+    const double v = partials[(long long)i * stride];
+    s = op_max ? fmax(s, v) : s + v;
+  }
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if (threadIdx.x < o) red[threadIdx.x] = op_max ? fmax(red[threadIdx.x], red[threadIdx.x + o])
+                                                   : red[threadIdx.x] + red[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *out = red[0];
+}
+
+// ------------------------------------------------------------------------------------
+// Host launchers.
+template <class K>
+static void set_smem(K kernel, size_t bytes) {
+  if (bytes > 48 * 1024) cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+template <int N>
+struct Launch {
+  static constexpr size_t yz_smem() { return (size_t)(N + kT * N) * sizeof(double2); }
+  static constexpr size_t x_smem(int nseq) { return (size_t)(N + nseq * row_pitch(N)) * sizeof(double2); }
+
+  static void zpass_inv_phase(const double2* u, double2* work, const double2* tw, const double2* phase, double scale,
+                              int ntiles, Geom g, cudaStream_t st) {
+    dim3 grid(ntiles, N, 3);
+    k_zpass_inv_phase<N><<<grid, nt_yz<N>(), yz_smem(), st>>>(u, work, tw, phase, scale, g);
+  }
+  static void ypass(double2* f, int nf, int dir, int ntiles, const double2* tw, Geom g, cudaStream_t st) {
+    dim3 grid(ntiles, N, nf);
+    if (dir < 0) {
+      k_ypass<N, -1><<<grid, nt_yz<N>(), yz_smem(), st>>>(f, tw, g);
+    } else {
+      k_ypass<N, +1><<<grid, nt_yz<N>(), yz_smem(), st>>>(f, tw, g);
+    }
+  }
+  static void zpass(const double2* src, double2* dst, int nf, int dir, int ntiles, double scale, const double2* tw,
+                    Geom g, cudaStream_t st) {
+    dim3 grid(ntiles, N, nf);
+    if (dir < 0) {
+      k_zpass<N, -1><<<grid, nt_yz<N>(), yz_smem(), st>>>(src, dst, scale, tw, g);
+    } else {
+      k_zpass<N, +1><<<grid, nt_yz<N>(), yz_smem(), st>>>(src, dst, scale, tw, g);
+    }
+  }
+  static void xpass_products(double2* work, const double2* unyq, const double2* phase, double scale, int nyq_scalar,
+                             double* partials, const double2* tw, Geom g, cudaStream_t st) {
+    k_xpass_products<N><<<N * N, nt_x<N>(), x_smem(6), st>>>(work, unyq, phase, scale, nyq_scalar, partials, tw, g);
+  }
+  static void nyq_reduce(const double2* work, double* sums, Geom g, cudaStream_t st) {
+    k_nyq_reduce<<<12, 256, 0, st>>>(work, sums, g);
+  }
+  static void sweep(const double2* work, double2* u, double2* gbuf, double2* rhs, const double* nyqsum,
+                    const double2* phase, SweepArgs a, Geom g, cudaStream_t st) {
+    const long long total = (long long)N * N * (N / 2);
+    k_sweep<N><<<(unsigned)((total + 255) / 256), 256, 0, st>>>(work, u, gbuf, rhs, nyqsum, phase, a, g);
+  }
+  static void xpass_r2c(const double* in, double2* out, int nf, const double2* tw, Geom g, cudaStream_t st) {
+    k_xpass_r2c<N><<<dim3(N * N / 2, nf), nt_x<N>(), x_smem(1), st>>>(in, out, tw, g);
+  }
+  static void xpass_c2r(const double2* in, double* out, int nf, const double2* tw, Geom g, cudaStream_t st) {
+    k_xpass_c2r<N><<<dim3(N * N / 2, nf), nt_x<N>(), x_smem(1), st>>>(in, out, tw, g);
+  }
+  static void xpass_diag(const double2* work, const double2* unyq, double scale, int nyq_scalar, double* partials,
+                         const double2* tw, Geom g, cudaStream_t st) {
+    k_xpass_diag<N><<<N * N, nt_x<N>(), x_smem(2), st>>>(work, unyq, scale, nyq_scalar, partials, tw, g);
+  }
+  // Opt every kernel of this size into its dynamic shared memory (once per process).
+  static void init() {
+    set_smem(k_zpass_inv_phase<N>, yz_smem());
+    set_smem(k_ypass<N, -1>, yz_smem());
+    set_smem(k_ypass<N, +1>, yz_smem());
+    set_smem(k_zpass<N, -1>, yz_smem());
+    set_smem(k_zpass<N, +1>, yz_smem());
+    set_smem(k_xpass_products<N>, x_smem(6));
+    set_smem(k_xpass_r2c<N>, x_smem(1));
+    set_smem(k_xpass_c2r<N>, x_smem(1));
+    set_smem(k_xpass_diag<N>, x_smem(2));
+  }
+  static const Ops* table() {
+    static const Ops ops = {N, init, zpass_inv_phase, ypass, zpass, xpass_products, nyq_reduce, sweep,
+                            xpass_r2c, xpass_c2r, xpass_diag};
+    return &ops;
+  }
+};
+
+const Ops* ops_for(int n) {
+  switch (n) {
+    case 8: return Launch<8>::table();
+    case 12: return Launch<12>::table();
+    case 16: return Launch<16>::table();
+    case 24: return Launch<24>::table();
+    case 32: return Launch<32>::table();
+    case 48: return Launch<48>::table();
+    case 64: return Launch<64>::table();
+    case 96: return Launch<96>::table();
+    case 128: return Launch<128>::table();
+    case 256: return Launch<256>::table();
+    case 512: return Launch<512>::table();
+    default: return nullptr;
+  }
+}
+
+static unsigned blocks_for(long long total, int bs) { return (unsigned)((total + bs - 1) / bs); }
+
+void launch_tgv_init(double* phys, Geom g, cudaStream_t st) {
+  const long long np = (long long)g.n * g.n * g.n;
+  k_tgv_init<<<blocks_for(np, 256), 256, 0, st>>>(phys, g.n);
+}
+void launch_project_truncate(double2* u, Geom g, cudaStream_t st) {
+  const long long total = (long long)g.n * g.n * (g.nh + 1);
+  k_project_truncate<<<blocks_for(total, 256), 256, 0, st>>>(u, g);
+}
+void launch_add_sparse(double2* u, const long long* idx, const double2* val, int count, cudaStream_t st) {
+  if (count > 0) k_add_sparse<<<blocks_for(count, 256), 256, 0, st>>>(u, idx, val, count);
+}
+void launch_half_to_full(const double2* half, double2* full, Geom g, cudaStream_t st) {
+  const long long total = (long long)g.n * g.n * g.n;
+  k_half_to_full<<<blocks_for(total, 256), 256, 0, st>>>(half, full, g);
+}
+void launch_full_to_half(const double2* full, double2* half, int hermitian_part, Geom g, cudaStream_t st) {
+  const long long total = (long long)g.n * g.n * (g.nh + 1);
+  k_full_to_half<<<blocks_for(total, 256), 256, 0, st>>>(full, half, hermitian_part, g);
+}
+void launch_spectral_diag(const double2* u, double* partials, int nblocks, Geom g, cudaStream_t st) {
+  k_spectral_diag<<<nblocks, 256, 0, st>>>(u, partials, g);
+}
+void launch_reduce(const double* partials, int count, int stride, int op_max, double* out, cudaStream_t st) {
+  k_reduce<<<1, 256, 0, st>>>(partials, count, stride, op_max, out);
+}
+
+}  // namespace sns
