@@ -10,6 +10,8 @@
 #include "sns_kernels.cuh"
 #include "../../include/sns_b200.h"
 
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -56,6 +58,11 @@ struct sns_handle {
   double* partials = nullptr;
   double* nyqsum = nullptr;
   double* red = nullptr;  // reduction results
+  int* err_word = nullptr;  // device error word written by bounded waits
+  int tma_grid = 0;         // persistent CTAs of the TMA passes
+  CUtensorMap map_state_z{};  // state fields (u[3], g[3]), z-pencil boxes
+  CUtensorMap map_work_y{};   // 12 work fields, y-pencil boxes
+  CUtensorMap map_work_z{};   // 12 work fields, z-pencil boxes
   size_t partial_count = 0;
   size_t bytes = 0;
   int fail_after = 0;
@@ -179,6 +186,50 @@ void perturbation_entries(int n, uint64_t seed, double amp, int kmax, const sns:
   }
 }
 
+using EncodeTiled = PFN_cuTensorMapEncodeTiled_v12000;
+
+EncodeTiled encode_fn() {
+  static EncodeTiled fn = nullptr;
+  if (fn == nullptr) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    ck(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q), "cudaGetDriverEntryPoint");
+    if (q != cudaDriverEntryPointSuccess || p == nullptr)
+      throw SnsError(SNS_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
+    fn = reinterpret_cast<EncodeTiled>(p);
+  }
+  return fn;
+}
+
+// Tensor map over `nf` consecutive half fields viewed as [field][z][y][2*pitch doubles],
+// box = 16 doubles (8 complex, 128 bytes) x up to 256 rows along y (axis 1) or z (axis 2).
+CUtensorMap make_field_map(void* base, int nf, int axis, const sns::Geom& g) {
+  CUtensorMap m;
+  const cuuint64_t row = (cuuint64_t)g.pitch * sizeof(double2);
+  cuuint64_t dims[4] = {(cuuint64_t)2 * g.pitch, (cuuint64_t)g.n, (cuuint64_t)g.n, (cuuint64_t)nf};
+  cuuint64_t strides[3] = {row, row * g.n, (cuuint64_t)g.field * sizeof(double2)};
+  const cuuint32_t br = g.n < 256 ? (cuuint32_t)g.n : 256u;
+  cuuint32_t box[4] = {16u, axis == 1 ? br : 1u, axis == 2 ? br : 1u, 1u};
+  cuuint32_t es[4] = {1u, 1u, 1u, 1u};
+  const CUresult r = encode_fn()(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, base, dims, strides, box, es,
+                                 CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                                 CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) throw SnsError(SNS_ERR_CUDA, "cuTensorMapEncodeTiled failed: " + std::to_string((int)r));
+  return m;
+}
+
+sns::TmaArgs tma_args(sns_handle* h, int f_in0, int nf, int ncb, double2* out, int f_out0, double scale) {
+  sns::TmaArgs a;
+  a.f_in0 = f_in0;
+  a.nf = nf;
+  a.ncb = ncb;
+  a.out = out;
+  a.f_out0 = f_out0;
+  a.scale = scale;
+  a.err = h->err_word;
+  return a;
+}
+
 void check_inject(sns_handle* h) {
   if (h->fail_after > 0) {
     if (--h->fail_after == 0) throw SnsError(SNS_ERR_INJECTED, "failure injected by sns_debug_fail_after");
@@ -188,6 +239,13 @@ void check_inject(sns_handle* h) {
 void sync(sns_handle* h, const char* what) {
   ck(cudaGetLastError(), what);
   ck(cudaStreamSynchronize(h->stream), what);
+  int e = 0;
+  ck(cudaMemcpy(&e, h->err_word, sizeof(int), cudaMemcpyDeviceToHost), what);
+  if (e != 0) {
+    cudaMemset(h->err_word, 0, sizeof(int));
+    throw SnsError(SNS_ERR_CUDA, std::string(what) + ": a pass gave up waiting for its TMA tile (code " +
+                                     std::to_string(e) + ")");
+  }
 }
 
 // Optional per-pass event marks (profiling entry point only).
@@ -207,18 +265,23 @@ void run_stage(sns_handle* h, double2* u_src, double2* g_buf, int stage, double 
   const sns::Geom& g = h->g;
   cudaStream_t st = h->stream;
   const int tiles_in = h->nyq_clean ? h->tiles_data() : h->tiles_all();
+  const int f_src = (int)((u_src - h->state) / g.field);  // u (0) or the g slot (3)
   mark(pm, 0, st);
-  o->zpass_inv_phase(u_src, h->work, h->tw, h->phase, h->inv_size(), tiles_in, g, st);
+  o->yz_tma(h->map_state_z, 2, +1, 1, tma_args(h, f_src, 3, tiles_in, h->work, 0, h->inv_size()), h->tw, h->phase,
+            g, h->tma_grid, st);
   mark(pm, 1, st);
-  o->ypass(h->work, 6, +1, tiles_in, h->tw, g, st);
+  o->yz_tma(h->map_work_y, 1, +1, 0, tma_args(h, 0, 6, tiles_in, h->work, 0, 1.0), h->tw, h->phase, g, h->tma_grid,
+            st);
   mark(pm, 2, st);
   o->xpass_products(h->work, u_src, h->phase, h->inv_size(), h->nyq_clean ? 1 : 0, partials, h->tw, g, st);
   mark(pm, 3, st);
   o->nyq_reduce(h->work, h->nyqsum, g, st);
   mark(pm, 4, st);
-  o->ypass(h->work, 12, -1, h->tiles_data(), h->tw, g, st);
+  o->yz_tma(h->map_work_y, 1, -1, 0, tma_args(h, 0, 12, h->tiles_data(), h->work, 0, 1.0), h->tw, h->phase, g,
+            h->tma_grid, st);
   mark(pm, 5, st);
-  o->zpass(h->work, h->work, 12, -1, h->tiles_data(), 1.0, h->tw, g, st);
+  o->yz_tma(h->map_work_z, 2, -1, 0, tma_args(h, 0, 12, h->tiles_data(), h->work, 0, 1.0), h->tw, h->phase, g,
+            h->tma_grid, st);
   mark(pm, 6, st);
   sns::SweepArgs a{};
   a.nu = h->nu;
@@ -279,8 +342,10 @@ void velocity_reductions(sns_handle* h) {
   const sns::Ops* o = h->ops;
   const sns::Geom& g = h->g;
   const int tiles = h->nyq_clean ? h->tiles_data() : h->tiles_all();
-  o->zpass(h->u(), h->work, 3, +1, tiles, h->inv_size(), h->tw, g, h->stream);
-  o->ypass(h->work, 3, +1, tiles, h->tw, g, h->stream);
+  o->yz_tma(h->map_state_z, 2, +1, 0, tma_args(h, 0, 3, tiles, h->work, 0, h->inv_size()), h->tw, h->phase, g,
+            h->tma_grid, h->stream);
+  o->yz_tma(h->map_work_y, 1, +1, 0, tma_args(h, 0, 3, tiles, h->work, 0, 1.0), h->tw, h->phase, g, h->tma_grid,
+            h->stream);
   o->xpass_diag(h->work, h->u(), h->inv_size(), h->nyq_clean ? 1 : 0, h->partials, h->tw, g, h->stream);
   const int rows = h->n * h->n;
   sns::launch_reduce(h->partials, rows, 2, 0, h->red + 0, h->stream);
@@ -319,6 +384,7 @@ void release(sns_handle* h) {
   cudaFree(h->partials);
   cudaFree(h->nyqsum);
   cudaFree(h->red);
+  cudaFree(h->err_word);
   if (h->ev0) cudaEventDestroy(h->ev0);
   if (h->ev1) cudaEventDestroy(h->ev1);
   if (h->stream) cudaStreamDestroy(h->stream);
@@ -414,6 +480,14 @@ int sns_create(int n, double nu, int precision, int viscous_mode, uint64_t seed,
     alloc((void**)&h->partials, h->partial_count * sizeof(double));
     alloc((void**)&h->nyqsum, 16 * sizeof(double));
     alloc((void**)&h->red, 16 * sizeof(double));
+    alloc((void**)&h->err_word, sizeof(int));
+    ck(cudaMemsetAsync(h->err_word, 0, sizeof(int), h->stream), "memset");
+    int nsm = 0;
+    ck(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device), "cudaDeviceGetAttribute");
+    h->tma_grid = nsm * ops->tma_blocks_per_sm();
+    h->map_state_z = make_field_map(h->state, 6, 2, h->g);
+    h->map_work_y = make_field_map(h->work, 12, 1, h->g);
+    h->map_work_z = make_field_map(h->work, 12, 2, h->g);
     ck(cudaMemsetAsync(h->state, 0, 6 * fb, h->stream), "memset");
     ck(cudaMemsetAsync(h->work, 0, 12 * fb, h->stream), "memset");
     const auto tw = twiddle_table(n);

@@ -21,11 +21,6 @@
 
 namespace sns {
 
-struct cplx_ops {
-  static __device__ __forceinline__ double2 add(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
-  static __device__ __forceinline__ double2 sub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
-};
-
 __device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
 __device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
@@ -211,6 +206,90 @@ __device__ __forceinline__ void fft_run(double2* buf, const double2* tw, int tid
 template <int L, int DIR, int NSEQ, int NT, class Addr>
 __device__ __forceinline__ void smem_fft(double2* buf, const double2* tw, int tid) {
   fft_run<L, DIR, NSEQ, NT, Addr>(buf, tw, tid, typename Plan<L>::type{});
+}
+
+
+// ------------------------------------------------------------------------------------
+// Tile FFT for the streaming y/z passes: 8 sequences (columns) of length L, element e of
+// column s at e*8 + s.  The first stage reads a source policy (the TMA-filled input
+// buffer, with any pre-multiplier fused into the load) and writes the work buffer W; the
+// middle stages run in place in W; the last stage writes a destination policy (global
+// memory, so the result never makes a second trip through shared memory).
+template <int L, int DIR, int NT, int Ns, int R, bool FIRST, bool LAST, class Src, class Dst>
+__device__ __forceinline__ void tstage(const Src& src, const Dst& dst, const double2* tw, int tid) {
+  constexpr int kBf = L / R;
+  constexpr int kTot = 8 * kBf;
+  constexpr int kBpt = (kTot + NT - 1) / NT;
+  constexpr int kTwStep = L / (Ns * R);
+  double2 v[kBpt][R];
+#pragma unroll
+  for (int i = 0; i < kBpt; ++i) {
+    const int b = tid + i * NT;
+    if (kTot % NT == 0 || b < kTot) {
+      const int s = b & 7, j = b >> 3;
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[i][r] = src(s, j + r * kBf);
+      if constexpr (Ns > 1) {
+        const int k = j % Ns;
+#pragma unroll
+        for (int r = 1; r < R; ++r) {
+          double2 w = tw[r * k * kTwStep];
+          if constexpr (DIR > 0) w.y = -w.y;
+          v[i][r] = cmul(v[i][r], w);
+        }
+      }
+      dftR<R, DIR>(v[i]);
+    }
+  }
+  if constexpr (!FIRST && !LAST) __syncthreads();  // in place in W
+#pragma unroll
+  for (int i = 0; i < kBpt; ++i) {
+    const int b = tid + i * NT;
+    if (kTot % NT == 0 || b < kTot) {
+      const int s = b & 7, j = b >> 3;
+      const int base = (j / Ns) * Ns * R + (j % Ns);
+#pragma unroll
+      for (int r = 0; r < R; ++r) dst(s, base + r * Ns, v[i][r]);
+    }
+  }
+  if constexpr (!LAST) __syncthreads();
+}
+
+struct WLoad {
+  const double2* w;
+  __device__ __forceinline__ double2 operator()(int s, int e) const { return w[e * 8 + s]; }
+};
+struct WStore {
+  double2* w;
+  __device__ __forceinline__ void operator()(int s, int e, double2 v) const { w[e * 8 + s] = v; }
+};
+
+template <int L, int DIR, int NT, int Ns, bool FIRST, class Src0, class DstG, int R, int... Rest>
+__device__ __forceinline__ void tfft_rec(const Src0& src0, double2* W, const DstG& dstg, const double2* tw, int tid) {
+  constexpr bool LAST = sizeof...(Rest) == 0;
+  if constexpr (FIRST && LAST) {
+    tstage<L, DIR, NT, Ns, R, true, true>(src0, dstg, tw, tid);
+  } else if constexpr (FIRST) {
+    tstage<L, DIR, NT, Ns, R, true, false>(src0, WStore{W}, tw, tid);
+  } else if constexpr (LAST) {
+    tstage<L, DIR, NT, Ns, R, false, true>(WLoad{W}, dstg, tw, tid);
+  } else {
+    tstage<L, DIR, NT, Ns, R, false, false>(WLoad{W}, WStore{W}, tw, tid);
+  }
+  if constexpr (!LAST) tfft_rec<L, DIR, NT, Ns * R, false, Src0, DstG, Rest...>(src0, W, dstg, tw, tid);
+}
+
+template <int L, int DIR, int NT, class Src0, class DstG, int... Rs>
+__device__ __forceinline__ void tfft_run(const Src0& src0, double2* W, const DstG& dstg, const double2* tw, int tid,
+                                         Radices<Rs...>) {
+  tfft_rec<L, DIR, NT, 1, true, Src0, DstG, Rs...>(src0, W, dstg, tw, tid);
+}
+
+// Transform the 8 columns read through src0; results go to dstg(s, e, value).  No barrier
+// is issued after the last stage: the caller syncs before reusing W or the source buffer.
+template <int L, int DIR, int NT, class Src0, class DstG>
+__device__ __forceinline__ void tile_fft(const Src0& src0, double2* W, const DstG& dstg, const double2* tw, int tid) {
+  tfft_run<L, DIR, NT>(src0, W, dstg, tw, tid, typename Plan<L>::type{});
 }
 
 }  // namespace sns

@@ -17,6 +17,7 @@
 // FFT with no r2c post-twiddle.
 #include "sns_fft.cuh"
 #include "sns_kernels.cuh"
+#include "sns_tma.cuh"
 
 #include <cstdio>
 
@@ -142,6 +143,131 @@ k_zpass(const double2* src, double2* dst, double scale, const double2* __restric
   for (int e = tid; e < kT * N; e += NT) {
     const int row = e / kT, col = e % kT;
     fout[((long long)row * N + y) * g.pitch + mx0 + col] = tile[e];
+  }
+}
+
+
+// ------------------------------------------------------------------------------------
+// Streaming y/z pass, persistent and TMA-fed.  Each CTA walks tiles (field, fixed
+// coordinate, 8-column block) with stride gridDim.x.  A tile (8 columns x N rows,
+// 128 bytes per row) lands in one of two shared-memory input buffers through
+// cp.async.bulk.tensor (no multicast) while the previous tile is transformed, so HBM
+// reads overlap the FFT.  The first radix stage reads the input buffer (scale and
+// phase shift fused into that read), middle stages run in a work buffer, and the last
+// stage stores straight to HBM as 128-byte row segments.
+// VARIANT 1 is the inverse z pass of u_hat with the phase shift: one read, two outputs
+// (U on field 2f and the shifted-grid V on field 2f+1).
+template <int N>
+constexpr int nt_tma() { return N < 64 ? 64 : (N > 512 ? 512 : N); }
+template <int N>
+constexpr int box_rows() { return N < 256 ? N : 256; }
+template <int N>
+constexpr size_t tma_smem() { return (size_t)(3 * 8 * N + N) * sizeof(double2) + 128 + 2 * sizeof(uint64_t); }
+// resident CTAs per SM the register budget is built for (shared memory allows this many)
+template <int N>
+constexpr int tma_minb() { return N >= 512 ? 1 : (N == 256 ? 2 : 4); }
+
+template <int N, int AXIS, int DIR, int VARIANT>
+__global__ void __launch_bounds__(nt_tma<N>(), tma_minb<N>())
+k_yz_tma(const __grid_constant__ CUtensorMap map, TmaArgs a, const double2* __restrict__ tw,
+         const double2* __restrict__ phase, Geom g) {
+  constexpr int NT = nt_tma<N>();
+  constexpr int BR = box_rows<N>();
+  constexpr int NBOX = N / BR;
+  constexpr uint32_t kTileBytes = 8u * N * sizeof(double2);
+  extern __shared__ unsigned char smraw[];
+  __shared__ int s_fail;
+  // 128-byte aligned layout: IN[0], IN[1], W (8N double2 each), twiddles (N), 2 mbarriers
+  const uint32_t pad = (128u - (smem_u32(smraw) & 127u)) & 127u;
+  double2* in0 = reinterpret_cast<double2*>(smraw + pad);
+  double2* in1 = in0 + 8 * N;
+  double2* W = in1 + 8 * N;
+  double2* s_tw = W + 8 * N;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(s_tw + N);
+  const int tid = threadIdx.x;
+  for (int t = tid; t < N; t += NT) s_tw[t] = tw[t];
+  const long long ntiles = (long long)a.nf * N * a.ncb;
+  if (tid == 0) {
+    mbar_init(&bars[0], 1);
+    mbar_init(&bars[1], 1);
+    fence_mbar_init();
+    s_fail = 0;
+  }
+  __syncthreads();
+  auto issue = [&](long long t, int b) {
+    const int cb = (int)(t % a.ncb);
+    const long long q = t / a.ncb;
+    const int c = (int)(q % N);
+    const int f = a.f_in0 + (int)(q / N);
+    double2* dst = b ? in1 : in0;
+    mbar_arrive_expect_tx(&bars[b], kTileBytes);
+#pragma unroll
+    for (int k = 0; k < NBOX; ++k) {
+      if constexpr (AXIS == 1) tma_load_4d(dst + k * BR * 8, &map, &bars[b], cb * 16, k * BR, c, f);
+      else tma_load_4d(dst + k * BR * 8, &map, &bars[b], cb * 16, c, k * BR, f);
+    }
+  };
+  long long t = blockIdx.x;
+  if (tid == 0) {
+    if (t < ntiles) issue(t, 0);
+    if (t + gridDim.x < ntiles) issue(t + gridDim.x, 1);
+  }
+  for (int k = 0; t < ntiles; ++k, t += gridDim.x) {
+    const int b = k & 1;
+    const uint32_t parity = (uint32_t)(k >> 1) & 1u;
+    if (tid == 0 && !mbar_wait_bounded(&bars[b], parity)) s_fail = 1;
+    __syncthreads();
+    if (s_fail) {
+      if (tid == 0) {
+        atomicExch(a.err, kErrTmaTimeout);
+        // let the other buffer's copy (if one is in flight) land before the CTA exits
+        (void)mbar_wait_bounded(&bars[b ^ 1], (uint32_t)((k + 1) >> 1) & 1u);
+      }
+      return;
+    }
+    (void)mbar_try_wait(&bars[b], parity);  // acquire the landed tile in every thread
+    const double2* IN = b ? in1 : in0;
+    const int cb = (int)(t % a.ncb);
+    const long long q = t / a.ncb;
+    const int c = (int)(q % N);
+    const int fi = (int)(q / N);
+    const int mx0 = cb * 8;
+    const double sc = a.scale;
+    if constexpr (VARIANT == 0) {
+      double2* outf = a.out + (long long)(a.f_out0 + fi) * g.field;
+      auto src = [&](int s, int e) {
+        const double2 v = IN[e * 8 + s];
+        return sc == 1.0 ? v : cscale(v, sc);
+      };
+      auto dst = [&](int s, int e, double2 v) {
+        const long long at = AXIS == 1 ? ((long long)c * N + e) * g.pitch : ((long long)e * N + c) * g.pitch;
+        outf[at + mx0 + s] = v;
+      };
+      tile_fft<N, DIR, NT>(src, W, dst, s_tw, tid);
+    } else {
+      static_assert(AXIS == 2, "phase variant is the inverse z pass");
+      double2* out_u = a.out + (long long)(a.f_out0 + 2 * fi) * g.field;
+      double2* out_v = out_u + g.field;
+      auto dst_u = [&](int s, int e, double2 v) { out_u[((long long)e * N + c) * g.pitch + mx0 + s] = v; };
+      auto dst_v = [&](int s, int e, double2 v) { out_v[((long long)e * N + c) * g.pitch + mx0 + s] = v; };
+      auto src_u = [&](int s, int e) { return cscale(IN[e * 8 + s], sc); };
+      tile_fft<N, DIR, NT>(src_u, W, dst_u, s_tw, tid);
+      __syncthreads();
+      const int smy = signed_mode(c, N);
+      auto src_v = [&](int s, int e) {
+        // shifted grid: phase exp(i*pi*(mx+my+mz)/N); modes with 0 < mx < N/2 and index N/2
+        // in exactly one of y, z are anti-Hermitian in the reference and drop out; columns
+        // past N/2 are padding
+        const int mx = mx0 + s;
+        const bool anti = mx > 0 && mx < N / 2 && ((c == N / 2) != (e == N / 2));
+        if (mx > N / 2 || anti) return make_double2(0.0, 0.0);
+        const double2 v = cscale(IN[e * 8 + s], sc);
+        return cmul(v, __ldg(&phase[mx + smy + signed_mode(e, N) + 3 * N / 2]));
+      };
+      tile_fft<N, DIR, NT>(src_v, W, dst_v, s_tw, tid);
+    }
+    __syncthreads();
+    if (tid == 0 && t + 2LL * gridDim.x < ntiles) issue(t + 2LL * gridDim.x, b);
   }
 }
 
@@ -786,8 +912,41 @@ struct Launch {
                          const double2* tw, Geom g, cudaStream_t st) {
     k_xpass_diag<N><<<N * N, nt_x<N>(), x_smem(2), st>>>(work, unyq, scale, nyq_scalar, partials, tw, g);
   }
+  template <int AXIS, int DIR, int VARIANT>
+  static void yz_tma_launch(const CUtensorMap& map, TmaArgs a, const double2* tw, const double2* phase, Geom g,
+                            int grid, cudaStream_t st) {
+    k_yz_tma<N, AXIS, DIR, VARIANT><<<grid, nt_tma<N>(), tma_smem<N>(), st>>>(map, a, tw, phase, g);
+  }
+  static void yz_tma(const CUtensorMap& map, int axis, int dir, int variant, TmaArgs a, const double2* tw,
+                     const double2* phase, Geom g, int grid, cudaStream_t st) {
+    if (variant == 1) yz_tma_launch<2, +1, 1>(map, a, tw, phase, g, grid, st);
+    else if (axis == 1 && dir < 0) yz_tma_launch<1, -1, 0>(map, a, tw, phase, g, grid, st);
+    else if (axis == 1) yz_tma_launch<1, +1, 0>(map, a, tw, phase, g, grid, st);
+    else if (dir < 0) yz_tma_launch<2, -1, 0>(map, a, tw, phase, g, grid, st);
+    else yz_tma_launch<2, +1, 0>(map, a, tw, phase, g, grid, st);
+  }
+  // Resident CTAs per SM of the TMA pass (all its instantiations share one footprint).
+  static int tma_blocks_per_sm() {
+    int lo = 1 << 30;
+    auto occ = [&](auto kernel) {
+      int nb = 0;
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel, nt_tma<N>(), tma_smem<N>());
+      lo = nb < lo ? nb : lo;
+    };
+    occ(k_yz_tma<N, 2, +1, 1>);
+    occ(k_yz_tma<N, 1, -1, 0>);
+    occ(k_yz_tma<N, 1, +1, 0>);
+    occ(k_yz_tma<N, 2, -1, 0>);
+    occ(k_yz_tma<N, 2, +1, 0>);
+    return lo > 0 && lo < (1 << 30) ? lo : 1;
+  }
   // Opt every kernel of this size into its dynamic shared memory (once per process).
   static void init() {
+    set_smem(k_yz_tma<N, 2, +1, 1>, tma_smem<N>());
+    set_smem(k_yz_tma<N, 1, -1, 0>, tma_smem<N>());
+    set_smem(k_yz_tma<N, 1, +1, 0>, tma_smem<N>());
+    set_smem(k_yz_tma<N, 2, -1, 0>, tma_smem<N>());
+    set_smem(k_yz_tma<N, 2, +1, 0>, tma_smem<N>());
     set_smem(k_zpass_inv_phase<N>, yz_smem());
     set_smem(k_ypass<N, -1>, yz_smem());
     set_smem(k_ypass<N, +1>, yz_smem());
@@ -800,7 +959,7 @@ struct Launch {
   }
   static const Ops* table() {
     static const Ops ops = {N, init, zpass_inv_phase, ypass, zpass, xpass_products, nyq_reduce, sweep,
-                            xpass_r2c, xpass_c2r, xpass_diag};
+                            xpass_r2c, xpass_c2r, xpass_diag, yz_tma, tma_blocks_per_sm};
     return &ops;
   }
 };

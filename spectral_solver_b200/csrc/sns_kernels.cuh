@@ -1,6 +1,7 @@
 // Kernel-side declarations shared by the pass kernels and the C-ABI host code.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <cstddef>
 #include <cstdint>
@@ -30,6 +31,17 @@ struct SweepArgs {
   int dealias;     // 1: phase-shift pair, 0: plain product only
 };
 
+// Arguments of the TMA-fed streaming y/z pass.
+struct TmaArgs {
+  int f_in0;      // first field of the tensor map to read
+  int nf;         // number of fields
+  int ncb;        // 8-column tiles per row
+  double2* out;   // output field set (field 0)
+  int f_out0;     // first output field (phase variant: 2 outputs per input field)
+  double scale;   // applied to every element on load
+  int* err;       // device error word (bounded-wait timeout)
+};
+
 // Launch table for one grid size.  All launches go to `st`.
 struct Ops {
   int n;
@@ -57,6 +69,10 @@ struct Ops {
   // physical velocity energy / vmax partials from 3 inverse-transformed fields
   void (*xpass_diag)(const double2* work, const double2* unyq, double scale, int nyq_scalar,
                      double* partials, const double2* tw, Geom g, cudaStream_t st);
+  // persistent TMA-fed y (axis 1) or z (axis 2) pass; variant 1 = inverse z with the phase shift
+  void (*yz_tma)(const CUtensorMap& map, int axis, int dir, int variant, TmaArgs a, const double2* tw,
+                 const double2* phase, Geom g, int grid, cudaStream_t st);
+  int (*tma_blocks_per_sm)();
 };
 
 const Ops* ops_for(int n);  // nullptr when the size has no FFT plan
