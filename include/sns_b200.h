@@ -86,6 +86,11 @@ int sns_get_state(sns_handle* h, double* const uhat_full[3]);
  * for the given state (full layout in and out).  The handle's own state is not changed. */
 int sns_rhs(sns_handle* h, const double* const uhat_full[3], double* const rhs_full[3]);
 
+/* Masked nonlinear term alone, -i k_j FFT(u_i u_j) dealiased and truncated, without the
+ * viscous term or the projection (SpectralNavierStokes::nonlinear_rhs,
+ * src/spectral_solver.cpp:160-240).  The handle's own state is not changed. */
+int sns_nonlinear(sns_handle* h, const double* const uhat_full[3], double* const out_full[3]);
+
 /* nsteps Williamson RK3 steps of size dt (TaylorGreenSolver::step_rk3, :979-1045). */
 int sns_step(sns_handle* h, double dt, int nsteps);
 
@@ -96,6 +101,10 @@ int sns_max_velocity(sns_handle* h, double* out);
 
 /* Final physical velocity: 3 arrays of N^3 doubles (the reference's layout). */
 int sns_dump_velocity(sns_handle* h, double* const phys[3]);
+
+/* Change the viscosity nu used by later RHS / step calls (SpectralNavierStokes passes its
+ * own viscosity to the backend's handle). */
+int sns_set_viscosity(sns_handle* h, double nu);
 
 /* Grid size and device bytes held by the handle. */
 int sns_grid_size(const sns_handle* h);

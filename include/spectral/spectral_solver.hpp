@@ -1,0 +1,109 @@
+// SpectralNavierStokes over the B200 backend: the reference's host-vector solver class
+// (src/spectral_solver.hpp:48-91 of ovankerm/Spectral_solver) with the same constructor,
+// methods, layouts and Diagnostics / SolverProfile records.
+//
+// The time step and the right-hand side run as fused sm_100a passes on the GPU
+// (rhs, nonlinear_rhs, step_rk3, the diagnostics); the pointwise helpers that take and
+// return host vectors (project, truncate, vorticity_hat, kinetic_energy of a physical
+// field) stay on the host as in the reference.  The fused passes need the reference's
+// benchmark domain: cubic grid, L = 2*pi on every axis (wavenumber = integer mode);
+// other domains throw std::runtime_error.
+#pragma once
+
+#include "spectral/b200_fft.hpp"
+
+#include <array>
+#include <complex>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace spectral {
+
+using ScalarPhysical = std::vector<double>;
+using ScalarSpectral = std::vector<double>;
+using VectorPhysical = std::array<ScalarPhysical, 3>;
+using VectorSpectral = std::array<ScalarSpectral, 3>;
+
+// The backend this build selects (the reference's `using FftBackend = ...`,
+// src/spectral_solver.hpp:19-23).
+using FftBackend = B200Fft3D;
+
+struct Diagnostics {
+  double t = 0.0;
+  double energy = 0.0;
+  double dissipation = 0.0;
+  double enstrophy = 0.0;
+  double max_spectral_divergence = 0.0;
+};
+
+struct SolverProfile {
+  double step_rk3 = 0.0;
+  double rhs = 0.0;
+  double nonlinear_rhs = 0.0;
+  double velocity_ifft = 0.0;
+  double shifted_velocity_ifft = 0.0;
+  double product_fft = 0.0;
+  double projection = 0.0;
+  double truncation = 0.0;
+  double diagnostics = 0.0;
+  int steps = 0;
+  int rhs_calls = 0;
+  int nonlinear_calls = 0;
+};
+
+class SpectralNavierStokes {
+ public:
+  SpectralNavierStokes(std::array<int, 3> shape, std::array<double, 3> lengths, double viscosity, MPI_Comm comm,
+                       bool phase_shift_dealiasing = true);
+  ~SpectralNavierStokes();
+
+  SpectralNavierStokes(const SpectralNavierStokes&) = delete;
+  SpectralNavierStokes& operator=(const SpectralNavierStokes&) = delete;
+
+  FftBackend& fft() { return fft_; }
+  const FftBackend& fft() const { return fft_; }
+
+  VectorPhysical taylor_green(double amplitude = 1.0, int mode = 1) const;
+  VectorSpectral to_spectral(const VectorPhysical& u);
+  VectorPhysical to_physical(const VectorSpectral& u_hat);
+
+  void project(VectorSpectral& u_hat) const;
+  void truncate(VectorSpectral& u_hat) const;
+  ScalarSpectral product_dealiased(const ScalarSpectral& a_hat, const ScalarSpectral& b_hat);
+  VectorSpectral nonlinear_rhs(const VectorSpectral& u_hat);
+  VectorSpectral rhs(const VectorSpectral& u_hat);
+  VectorSpectral step_rk3(const VectorSpectral& u_hat, double t, double dt);
+
+  double kinetic_energy(const VectorPhysical& u) const;
+  double kinetic_energy_spectral(const VectorSpectral& u_hat);
+  double max_velocity(const VectorSpectral& u_hat);
+  VectorSpectral vorticity_hat(const VectorSpectral& u_hat) const;
+  double enstrophy(const VectorSpectral& u_hat);
+  double dissipation(const VectorSpectral& u_hat);
+  double max_spectral_divergence(const VectorSpectral& u_hat) const;
+  Diagnostics diagnostics(const VectorSpectral& u_hat, double t);
+  void reset_profile();
+  const SolverProfile& profile() const { return profile_; }
+
+ private:
+  bool keep_mode(const SpectralMode& mode) const;
+  void zero_mean(VectorSpectral& u_hat) const;
+  sns_handle* solver_handle();
+  void require_device_domain() const;
+  struct DeviceDiag;
+  DeviceDiag device_diagnostics(const VectorSpectral& u_hat);
+
+  FftBackend fft_;
+  double nu_ = 0.0;
+  bool phase_shift_dealiasing_ = true;
+  std::vector<std::complex<double>> phase_shift_;
+  std::vector<std::uint8_t> keep_mode_mask_;
+  SolverProfile profile_;
+  sns_handle* solver_ = nullptr;  // fused-pass handle (created on first use)
+};
+
+void write_diagnostics_csv(const std::string& path, const std::vector<Diagnostics>& history);
+void write_vorticity_ppm(const std::string& path, SpectralNavierStokes& solver, const VectorSpectral& u_hat);
+
+}  // namespace spectral

@@ -50,10 +50,12 @@ SIGNATURES = {
     "sns_set_state": (C.c_int, [_H, _DPP]),
     "sns_get_state": (C.c_int, [_H, _DPP]),
     "sns_rhs": (C.c_int, [_H, _DPP, _DPP]),
+    "sns_nonlinear": (C.c_int, [_H, _DPP, _DPP]),
     "sns_step": (C.c_int, [_H, C.c_double, C.c_int]),
     "sns_diagnostics": (C.c_int, [_H, C.c_double, C.POINTER(SnsDiag)]),
     "sns_max_velocity": (C.c_int, [_H, _DP]),
     "sns_dump_velocity": (C.c_int, [_H, _DPP]),
+    "sns_set_viscosity": (C.c_int, [_H, C.c_double]),
     "sns_grid_size": (C.c_int, [_H]),
     "sns_device_bytes": (C.c_size_t, [_H]),
     "sns_time_steps": (C.c_int, [_H, C.c_double, C.c_int, _DP]),
@@ -172,6 +174,13 @@ class Solver:
         ins = [full_to_interleaved(c) for c in u_full]
         outs = [np.empty(2 * n ** 3, np.float64) for _ in range(3)]
         self._check(self.lib.sns_rhs(self.h, _arr3(ins), _arr3(outs)))
+        return [interleaved_to_full(a, n) for a in outs]
+
+    def nonlinear(self, u_full):
+        n = self.n
+        ins = [full_to_interleaved(c) for c in u_full]
+        outs = [np.empty(2 * n ** 3, np.float64) for _ in range(3)]
+        self._check(self.lib.sns_nonlinear(self.h, _arr3(ins), _arr3(outs)))
         return [interleaved_to_full(a, n) for a in outs]
 
     def step(self, dt: float, nsteps: int = 1):

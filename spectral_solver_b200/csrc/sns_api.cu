@@ -538,6 +538,16 @@ const char* sns_last_error(const sns_handle* h) {
   return h->err.c_str();
 }
 
+int sns_set_viscosity(sns_handle* h, double nu) {
+  if (h == nullptr) return SNS_ERR_INVALID;
+  if (!(nu >= 0.0) || !std::isfinite(nu)) {
+    h->err = "viscosity must be finite and non-negative";
+    return SNS_ERR_INVALID;
+  }
+  h->nu = nu;
+  return SNS_OK;
+}
+
 int sns_grid_size(const sns_handle* h) { return h ? h->n : 0; }
 size_t sns_device_bytes(const sns_handle* h) { return h ? h->bytes : 0; }
 
@@ -620,6 +630,30 @@ int sns_rhs(sns_handle* h, const double* const uhat_full[3], double* const rhs_f
     for (int c = 0; c < 3; ++c) {
       download_full(h, h->wf(c), rhs_full[c]);
       sync(h, "sns_rhs");
+    }
+  });
+}
+
+int sns_nonlinear(sns_handle* h, const double* const uhat_full[3], double* const out_full[3]) {
+  return guarded(h, [&] {
+    if (!uhat_full || !out_full) throw SnsError(SNS_ERR_INVALID, "null buffer");
+    for (int c = 0; c < 3; ++c)
+      if (!uhat_full[c] || !out_full[c]) throw SnsError(SNS_ERR_INVALID, "null buffer");
+    double2* uin = h->gb();
+    ck(cudaMemsetAsync(uin, 0, 3 * field_bytes(h->n), h->stream), "memset");
+    bool dirty = false;
+    for (int c = 0; c < 3; ++c) {
+      upload_full(h, uhat_full[c], uin + (long long)c * h->g.field, 0);
+      dirty = dirty || nyquist_plane_dirty(h->n, uhat_full[c]);
+      sync(h, "sns_nonlinear upload");
+    }
+    const bool saved = h->nyq_clean;
+    h->nyq_clean = !dirty;
+    run_stage(h, uin, nullptr, 0, 0.0, 2, h->work, nullptr);
+    h->nyq_clean = saved;
+    for (int c = 0; c < 3; ++c) {
+      download_full(h, h->wf(c), out_full[c]);
+      sync(h, "sns_nonlinear");
     }
   });
 }

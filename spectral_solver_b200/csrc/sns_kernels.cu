@@ -439,6 +439,12 @@ __device__ __forceinline__ void sweep_mode(const ModeIn& in, int ix, int iy, int
     if (pa[p] != pb[p]) r[pb[p]] = cadd(r[pb[p]], minus_i_k(value, kv[pa[p]]));
   }
   const double k2 = (double)m2;
+  if (a.mode == 2) {  // nonlinear term only: masked, neither viscous term nor projection
+    rr[0] = r[0];
+    rr[1] = r[1];
+    rr[2] = r[2];
+    return;
+  }
 #pragma unroll
   for (int c = 0; c < 3; ++c) r[c] = csub(r[c], cscale(uu[c], a.nu * k2));
   if (k2 > 0.0 && keep) {
@@ -500,7 +506,7 @@ k_sweep(const double2* __restrict__ work, double2* __restrict__ u, double2* __re
       gg[c] = load_g ? gbuf[(long long)c * g.field + idx] : make_double2(0, 0);
     }
     sweep_mode(in, mx, my, mz, N, phase[mx + my + mz + 3 * N / 2], uu, gg, load_g, rr, a);
-    if (a.mode == 1) {
+    if (a.mode != 0) {
 #pragma unroll
       for (int c = 0; c < 3; ++c) rhs[(long long)c * g.field + idx] = rr[c];
     } else {
@@ -517,7 +523,7 @@ k_sweep(const double2* __restrict__ work, double2* __restrict__ u, double2* __re
       const double2 zero = make_double2(0.0, 0.0);
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
-        if (a.mode == 1) {
+        if (a.mode != 0) {
           rhs[(long long)c * g.field + inq] = zero;
         } else {
           u[(long long)c * g.field + inq] = zero;
@@ -542,7 +548,7 @@ k_sweep(const double2* __restrict__ work, double2* __restrict__ u, double2* __re
       gg[c] = load_g ? gbuf[(long long)c * g.field + idx] : make_double2(0, 0);
     }
     sweep_mode(in, NH, 0, 0, N, phase[NH + 3 * N / 2], uu, gg, load_g, rr, a);
-    if (a.mode == 1) {
+    if (a.mode != 0) {
 #pragma unroll
       for (int c = 0; c < 3; ++c) rhs[(long long)c * g.field + idx] = rr[c];
     } else {

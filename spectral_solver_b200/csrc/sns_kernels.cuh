@@ -27,7 +27,7 @@ struct SweepArgs {
   double ga;       // g <- ga*g + r   (stage 1: unused, g <- r)
   double ub;       // u <- u + ub*g
   int stage;       // 0, 1, 2
-  int mode;        // 0: RK update of (u, g); 1: write the projected RHS to `rhs`
+  int mode;        // 0: RK update of (u, g); 1: projected RHS to `rhs`; 2: masked nonlinear term only
   int dealias;     // 1: phase-shift pair, 0: plain product only
 };
 

@@ -1,0 +1,294 @@
+// SpectralNavierStokes over B200Fft3D (the reference's src/spectral_solver.cpp:35-488 API).
+//
+// rhs / nonlinear_rhs / step_rk3 / the spectral diagnostics go through the fused device
+// passes of the backend's handle; host-vector helpers keep the reference's semantics.
+#include "spectral/spectral_solver.hpp"
+
+#include "sns_b200.h"
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <fstream>
+#include <iomanip>
+#include <stdexcept>
+
+namespace spectral {
+
+namespace {
+
+constexpr double kPi = 3.141592653589793238462643383279502884;
+using Clock = std::chrono::steady_clock;
+
+double seconds_since(Clock::time_point t0) { return std::chrono::duration<double>(Clock::now() - t0).count(); }
+
+std::complex<double> at(const std::vector<double>& a, std::size_t id) { return {a[id], a[id + 1]}; }
+void put(std::vector<double>& a, std::size_t id, std::complex<double> z) {
+  a[id] = z.real();
+  a[id + 1] = z.imag();
+}
+
+void check(int rc, sns_handle* h, const char* what) {
+  if (rc != SNS_OK) throw std::runtime_error(std::string(what) + ": " + sns_last_error(h));
+}
+
+VectorSpectral zeros_spectral(std::size_t n) { return {ScalarSpectral(n, 0.0), ScalarSpectral(n, 0.0), ScalarSpectral(n, 0.0)}; }
+
+}  // namespace
+
+struct SpectralNavierStokes::DeviceDiag {
+  sns_diag d;
+};
+
+SpectralNavierStokes::SpectralNavierStokes(std::array<int, 3> shape, std::array<double, 3> lengths, double viscosity,
+                                           MPI_Comm comm, bool phase_shift_dealiasing)
+    : fft_(shape, lengths, comm), nu_(viscosity), phase_shift_dealiasing_(phase_shift_dealiasing) {
+  if (nu_ < 0.0) throw std::runtime_error("viscosity must be non-negative");
+  const std::size_t nmodes = fft_.spectral_storage_size() / 2;
+  phase_shift_.resize(nmodes);
+  keep_mode_mask_.resize(nmodes);
+  const auto& L = fft_.lengths();
+  const auto& n = fft_.shape();
+  // half-cell shift dx = L/(2n) on every axis, as src/spectral_solver.cpp:48-54
+  const double hx = 0.5 * L[0] / n[0], hy = 0.5 * L[1] / n[1], hz = 0.5 * L[2] / n[2];
+  fft_.for_each_spectral([&](std::size_t id, const SpectralMode& m) {
+    phase_shift_[id / 2] = std::exp(std::complex<double>(0.0, m.kx * hx + m.ky * hy + m.kz * hz));
+    keep_mode_mask_[id / 2] = keep_mode(m) ? 1 : 0;
+  });
+}
+
+SpectralNavierStokes::~SpectralNavierStokes() = default;
+
+void SpectralNavierStokes::require_device_domain() const {
+  const auto& L = fft_.lengths();
+  for (double l : L) {
+    if (std::abs(l - 2.0 * kPi) > 1e-12 * 2.0 * kPi)
+      throw std::runtime_error("the fused B200 passes need the [0, 2*pi)^3 domain (wavenumber = integer mode)");
+  }
+  if (!phase_shift_dealiasing_)
+    throw std::runtime_error("the fused B200 passes implement the phase-shift dealiased product");
+}
+
+sns_handle* SpectralNavierStokes::solver_handle() {
+  require_device_domain();
+  sns_handle* h = fft_.handle();
+  check(sns_set_viscosity(h, nu_), h, "SpectralNavierStokes");
+  return h;
+}
+
+VectorPhysical SpectralNavierStokes::taylor_green(double amplitude, int mode) const {
+  const auto& n = fft_.shape();
+  const auto& L = fft_.lengths();
+  const std::size_t np = static_cast<std::size_t>(fft_.physical_size());
+  VectorPhysical u = {ScalarPhysical(np, 0.0), ScalarPhysical(np, 0.0), ScalarPhysical(np, 0.0)};
+  fft_.for_each_physical([&](std::size_t id, int ix, int iy, int iz) {
+    const double ax = 2.0 * kPi * mode * ((ix + 0.5) * L[0] / n[0]) / L[0];
+    const double ay = 2.0 * kPi * mode * ((iy + 0.5) * L[1] / n[1]) / L[1];
+    const double az = 2.0 * kPi * mode * ((iz + 0.5) * L[2] / n[2]) / L[2];
+    u[0][id] = amplitude * std::sin(ax) * std::cos(ay) * std::cos(az);
+    u[1][id] = -amplitude * std::cos(ax) * std::sin(ay) * std::cos(az);
+  });
+  return u;
+}
+
+VectorSpectral SpectralNavierStokes::to_spectral(const VectorPhysical& u) {
+  VectorSpectral out;
+  for (int c = 0; c < 3; ++c) out[c] = fft_.forward(u[c]);
+  return out;
+}
+
+VectorPhysical SpectralNavierStokes::to_physical(const VectorSpectral& u_hat) {
+  VectorPhysical out;
+  for (int c = 0; c < 3; ++c) out[c] = fft_.backward(u_hat[c]);
+  return out;
+}
+
+void SpectralNavierStokes::project(VectorSpectral& u_hat) const {
+  fft_.for_each_spectral([&](std::size_t id, const SpectralMode& m) {
+    if (m.k2 == 0.0) return;
+    const auto ux = at(u_hat[0], id), uy = at(u_hat[1], id), uz = at(u_hat[2], id);
+    const auto f = (m.kx * ux + m.ky * uy + m.kz * uz) / m.k2;
+    put(u_hat[0], id, ux - m.kx * f);
+    put(u_hat[1], id, uy - m.ky * f);
+    put(u_hat[2], id, uz - m.kz * f);
+  });
+  zero_mean(u_hat);
+}
+
+void SpectralNavierStokes::truncate(VectorSpectral& u_hat) const {
+  fft_.for_each_spectral([&](std::size_t id, const SpectralMode&) {
+    if (keep_mode_mask_[id / 2]) return;
+    for (auto& comp : u_hat) comp[id] = comp[id + 1] = 0.0;
+  });
+}
+
+ScalarSpectral SpectralNavierStokes::product_dealiased(const ScalarSpectral& a_hat, const ScalarSpectral& b_hat) {
+  // device transforms; the two products and the combine are pointwise host work, as in
+  // src/spectral_solver.cpp:122-158
+  const auto a = fft_.backward(a_hat);
+  const auto b = fft_.backward(b_hat);
+  ScalarPhysical p(a.size());
+  for (std::size_t i = 0; i < p.size(); ++i) p[i] = a[i] * b[i];
+  const auto c0 = fft_.forward(p);
+  ScalarSpectral as = a_hat, bs = b_hat;
+  for (std::size_t m = 0; m < phase_shift_.size(); ++m) {
+    put(as, 2 * m, at(as, 2 * m) * phase_shift_[m]);
+    put(bs, 2 * m, at(bs, 2 * m) * phase_shift_[m]);
+  }
+  const auto sa = fft_.backward(as);
+  const auto sb = fft_.backward(bs);
+  for (std::size_t i = 0; i < p.size(); ++i) p[i] = sa[i] * sb[i];
+  const auto cs = fft_.forward(p);
+  ScalarSpectral out(c0.size(), 0.0);
+  for (std::size_t m = 0; m < phase_shift_.size(); ++m) {
+    if (!keep_mode_mask_[m]) continue;
+    put(out, 2 * m, 0.5 * (at(c0, 2 * m) + at(cs, 2 * m) * std::conj(phase_shift_[m])));
+  }
+  return out;
+}
+
+VectorSpectral SpectralNavierStokes::nonlinear_rhs(const VectorSpectral& u_hat) {
+  const auto t0 = Clock::now();
+  profile_.nonlinear_calls += 1;
+  sns_handle* h = solver_handle();
+  VectorSpectral out = zeros_spectral(fft_.spectral_storage_size());
+  const double* in[3] = {u_hat[0].data(), u_hat[1].data(), u_hat[2].data()};
+  double* o[3] = {out[0].data(), out[1].data(), out[2].data()};
+  check(sns_nonlinear(h, in, o), h, "SpectralNavierStokes::nonlinear_rhs");
+  profile_.nonlinear_rhs += seconds_since(t0);
+  return out;
+}
+
+VectorSpectral SpectralNavierStokes::rhs(const VectorSpectral& u_hat) {
+  const auto t0 = Clock::now();
+  profile_.rhs_calls += 1;
+  sns_handle* h = solver_handle();
+  VectorSpectral out = zeros_spectral(fft_.spectral_storage_size());
+  const double* in[3] = {u_hat[0].data(), u_hat[1].data(), u_hat[2].data()};
+  double* o[3] = {out[0].data(), out[1].data(), out[2].data()};
+  check(sns_rhs(h, in, o), h, "SpectralNavierStokes::rhs");
+  profile_.rhs += seconds_since(t0);
+  return out;
+}
+
+VectorSpectral SpectralNavierStokes::step_rk3(const VectorSpectral& u_hat, double t, double dt) {
+  (void)t;
+  const auto t0 = Clock::now();
+  profile_.steps += 1;
+  sns_handle* h = solver_handle();
+  const double* in[3] = {u_hat[0].data(), u_hat[1].data(), u_hat[2].data()};
+  check(sns_set_state(h, in), h, "SpectralNavierStokes::step_rk3");
+  check(sns_step(h, dt, 1), h, "SpectralNavierStokes::step_rk3");
+  VectorSpectral out = zeros_spectral(fft_.spectral_storage_size());
+  double* o[3] = {out[0].data(), out[1].data(), out[2].data()};
+  check(sns_get_state(h, o), h, "SpectralNavierStokes::step_rk3");
+  profile_.step_rk3 += seconds_since(t0);
+  return out;
+}
+
+double SpectralNavierStokes::kinetic_energy(const VectorPhysical& u) const {
+  double sum = 0.0;
+  for (std::size_t i = 0; i < u[0].size(); ++i) sum += 0.5 * (u[0][i] * u[0][i] + u[1][i] * u[1][i] + u[2][i] * u[2][i]);
+  double total = 0.0;
+  MPI_Allreduce(&sum, &total, 1, MPI_DOUBLE, MPI_SUM, fft_.comm());
+  return total / static_cast<double>(fft_.global_physical_size());
+}
+
+SpectralNavierStokes::DeviceDiag SpectralNavierStokes::device_diagnostics(const VectorSpectral& u_hat) {
+  sns_handle* h = solver_handle();
+  const double* in[3] = {u_hat[0].data(), u_hat[1].data(), u_hat[2].data()};
+  check(sns_set_state(h, in), h, "SpectralNavierStokes diagnostics");
+  DeviceDiag d{};
+  check(sns_diagnostics(h, 0.0, &d.d), h, "SpectralNavierStokes diagnostics");
+  return d;
+}
+
+double SpectralNavierStokes::kinetic_energy_spectral(const VectorSpectral& u_hat) {
+  return device_diagnostics(u_hat).d.kinetic_energy;
+}
+
+double SpectralNavierStokes::max_velocity(const VectorSpectral& u_hat) {
+  return device_diagnostics(u_hat).d.max_velocity;
+}
+
+VectorSpectral SpectralNavierStokes::vorticity_hat(const VectorSpectral& u_hat) const {
+  VectorSpectral w = zeros_spectral(fft_.spectral_storage_size());
+  const std::complex<double> I(0.0, 1.0);
+  fft_.for_each_spectral([&](std::size_t id, const SpectralMode& m) {
+    const auto ux = at(u_hat[0], id), uy = at(u_hat[1], id), uz = at(u_hat[2], id);
+    put(w[0], id, I * (m.ky * uz - m.kz * uy));
+    put(w[1], id, I * (m.kz * ux - m.kx * uz));
+    put(w[2], id, I * (m.kx * uy - m.ky * ux));
+  });
+  return w;
+}
+
+double SpectralNavierStokes::enstrophy(const VectorSpectral& u_hat) { return device_diagnostics(u_hat).d.enstrophy; }
+
+double SpectralNavierStokes::dissipation(const VectorSpectral& u_hat) { return 2.0 * nu_ * enstrophy(u_hat); }
+
+double SpectralNavierStokes::max_spectral_divergence(const VectorSpectral& u_hat) const {
+  double mx = 0.0;
+  fft_.for_each_spectral([&](std::size_t id, const SpectralMode& m) {
+    mx = std::max(mx, std::abs(m.kx * at(u_hat[0], id) + m.ky * at(u_hat[1], id) + m.kz * at(u_hat[2], id)));
+  });
+  double total = 0.0;
+  MPI_Allreduce(&mx, &total, 1, MPI_DOUBLE, MPI_MAX, fft_.comm());
+  return total;
+}
+
+Diagnostics SpectralNavierStokes::diagnostics(const VectorSpectral& u_hat, double t) {
+  const auto t0 = Clock::now();
+  const auto d = device_diagnostics(u_hat).d;
+  Diagnostics row{t, d.kinetic_energy, 2.0 * nu_ * d.enstrophy, d.enstrophy, d.max_spectral_divergence};
+  profile_.diagnostics += seconds_since(t0);
+  return row;
+}
+
+void SpectralNavierStokes::reset_profile() { profile_ = SolverProfile{}; }
+
+bool SpectralNavierStokes::keep_mode(const SpectralMode& m) const {
+  const auto& n = fft_.shape();
+  const double hx = n[0] / 2.0, hy = n[1] / 2.0, hz = n[2] / 2.0;
+  return (m.mx * m.mx) / (hx * hx) + (m.my * m.my) / (hy * hy) + (m.mz * m.mz) / (hz * hz) <= 1.0;
+}
+
+void SpectralNavierStokes::zero_mean(VectorSpectral& u_hat) const {
+  for (auto& comp : u_hat) comp[0] = comp[1] = 0.0;  // mode (0,0,0) sits at index 0
+}
+
+void write_diagnostics_csv(const std::string& path, const std::vector<Diagnostics>& history) {
+  std::ofstream f(path);
+  f << "t,kinetic_energy,dissipation,enstrophy,max_spectral_divergence\n" << std::setprecision(17);
+  for (const auto& r : history)
+    f << r.t << ',' << r.energy << ',' << r.dissipation << ',' << r.enstrophy << ',' << r.max_spectral_divergence << '\n';
+}
+
+void write_vorticity_ppm(const std::string& path, SpectralNavierStokes& solver, const VectorSpectral& u_hat) {
+  // |omega| on the mid z plane as a binary PPM (src/spectral_solver.cpp:421-486)
+  const auto w = solver.to_physical(solver.vorticity_hat(u_hat));
+  const auto& n = solver.fft().shape();
+  const int iz = n[2] / 2;
+  std::vector<double> mag(static_cast<std::size_t>(n[0]) * n[1]);
+  double vmax = 0.0;
+  for (int iy = 0; iy < n[1]; ++iy)
+    for (int ix = 0; ix < n[0]; ++ix) {
+      const std::size_t src = static_cast<std::size_t>(ix + n[0] * (iy + n[1] * iz));
+      const double v = std::sqrt(w[0][src] * w[0][src] + w[1][src] * w[1][src] + w[2][src] * w[2][src]);
+      mag[static_cast<std::size_t>(ix + n[0] * iy)] = v;
+      vmax = std::max(vmax, v);
+    }
+  if (vmax == 0.0) vmax = 1.0;
+  std::ofstream f(path, std::ios::binary);
+  f << "P6\n" << n[0] << " " << n[1] << "\n255\n";
+  for (int iy = n[1] - 1; iy >= 0; --iy)
+    for (int ix = 0; ix < n[0]; ++ix) {
+      const double q = std::clamp(mag[static_cast<std::size_t>(ix + n[0] * iy)] / vmax, 0.0, 1.0);
+      const unsigned char rgb[3] = {static_cast<unsigned char>(255.0 * std::sqrt(q)),
+                                    static_cast<unsigned char>(255.0 * q * q),
+                                    static_cast<unsigned char>(255.0 * (1.0 - q) * 0.25)};
+      f.write(reinterpret_cast<const char*>(rgb), 3);
+    }
+}
+
+}  // namespace spectral
