@@ -56,10 +56,13 @@ struct sns_handle {
   double2* tw = nullptr;
   double2* phase = nullptr;
   double* partials = nullptr;
-  double* nyqsum = nullptr;
   double* red = nullptr;  // reduction results
   int* err_word = nullptr;  // device error word written by bounded waits
   int tma_grid = 0;         // persistent CTAs of the TMA passes
+  int x2_grid = 0;          // persistent CTAs of the two-stage x pass (0: generic x pass)
+  int p5_grid = 0;          // persistent CTAs of the fused forward-z + sweep pass (0: two kernels)
+  double2* tw2 = nullptr;   // W_N^(r*j), r < N/16, j < 16 (two-stage x pass)
+  double* nyq_part = nullptr;  // [12][max(1, x2_grid)] Nyquist-plane partial sums
   CUtensorMap map_state_z{};  // state fields (u[3], g[3]), z-pencil boxes
   CUtensorMap map_work_y{};   // 12 work fields, y-pencil boxes
   CUtensorMap map_work_z{};   // 12 work fields, z-pencil boxes
@@ -273,15 +276,25 @@ void run_stage(sns_handle* h, double2* u_src, double2* g_buf, int stage, double 
   o->yz_tma(h->map_work_y, 1, +1, 0, tma_args(h, 0, 6, tiles_in, h->work, 0, 1.0), h->tw, h->phase, g, h->tma_grid,
             st);
   mark(pm, 2, st);
-  o->xpass_products(h->work, u_src, h->phase, h->inv_size(), h->nyq_clean ? 1 : 0, partials, h->tw, g, st);
-  mark(pm, 3, st);
-  o->nyq_reduce(h->work, h->nyqsum, g, st);
+  int nparts = 1;
+  if (h->x2_grid > 0 && partials == nullptr) {
+    o->xpass2(h->work, u_src, h->phase, h->inv_size(), h->nyq_clean ? 1 : 0, h->nyq_part, h->tw2, g, h->x2_grid,
+              h->err_word, st);
+    nparts = h->x2_grid;
+    mark(pm, 3, st);
+  } else {
+    o->xpass_products(h->work, u_src, h->phase, h->inv_size(), h->nyq_clean ? 1 : 0, partials, h->tw, g, st);
+    mark(pm, 3, st);
+    o->nyq_reduce(h->work, h->nyq_part, g, st);
+  }
   mark(pm, 4, st);
   o->yz_tma(h->map_work_y, 1, -1, 0, tma_args(h, 0, 12, h->tiles_data(), h->work, 0, 1.0), h->tw, h->phase, g,
             h->tma_grid, st);
   mark(pm, 5, st);
-  o->yz_tma(h->map_work_z, 2, -1, 0, tma_args(h, 0, 12, h->tiles_data(), h->work, 0, 1.0), h->tw, h->phase, g,
-            h->tma_grid, st);
+  const bool fused = h->p5_grid > 0;
+  if (!fused)
+    o->yz_tma(h->map_work_z, 2, -1, 0, tma_args(h, 0, 12, h->tiles_data(), h->work, 0, 1.0), h->tw, h->phase, g,
+              h->tma_grid, st);
   mark(pm, 6, st);
   sns::SweepArgs a{};
   a.nu = h->nu;
@@ -298,7 +311,11 @@ void run_stage(sns_handle* h, double2* u_src, double2* g_buf, int stage, double 
     a.ga = -153.0 / 128.0;
     a.ub = 8.0 * dt / 15.0;
   }
-  o->sweep(h->work, u_src, g_buf, rhs_out, h->nyqsum, h->phase, a, g, st);
+  if (fused)
+    o->p5(h->map_work_z, u_src, g_buf, rhs_out, h->nyq_part, nparts, h->tw, h->phase, a, h->tiles_data(), g,
+          h->p5_grid, h->err_word, st);
+  else
+    o->sweep(h->work, u_src, g_buf, rhs_out, h->nyq_part, nparts, h->phase, a, g, st);
   mark(pm, 7, st);
 }
 
@@ -382,9 +399,10 @@ void release(sns_handle* h) {
   cudaFree(h->tw);
   cudaFree(h->phase);
   cudaFree(h->partials);
-  cudaFree(h->nyqsum);
   cudaFree(h->red);
   cudaFree(h->err_word);
+  cudaFree(h->tw2);
+  cudaFree(h->nyq_part);
   if (h->ev0) cudaEventDestroy(h->ev0);
   if (h->ev1) cudaEventDestroy(h->ev1);
   if (h->stream) cudaStreamDestroy(h->stream);
@@ -478,13 +496,24 @@ int sns_create(int n, double nu, int precision, int viscous_mode, uint64_t seed,
     alloc((void**)&h->tw, (size_t)n * sizeof(double2));
     alloc((void**)&h->phase, (size_t)(3 * n + 1) * sizeof(double2));
     alloc((void**)&h->partials, h->partial_count * sizeof(double));
-    alloc((void**)&h->nyqsum, 16 * sizeof(double));
     alloc((void**)&h->red, 16 * sizeof(double));
     alloc((void**)&h->err_word, sizeof(int));
     ck(cudaMemsetAsync(h->err_word, 0, sizeof(int), h->stream), "memset");
     int nsm = 0;
     ck(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device), "cudaDeviceGetAttribute");
     h->tma_grid = nsm * ops->tma_blocks_per_sm();
+    h->x2_grid = ops->xpass2_grid(nsm);
+    h->p5_grid = ops->p5_grid(nsm);
+    alloc((void**)&h->nyq_part, (size_t)12 * (h->x2_grid > 0 ? h->x2_grid : 1) * sizeof(double));
+    alloc((void**)&h->tw2, (size_t)n * sizeof(double2));
+    {
+      // tw2[r*16 + j] = exp(-2*pi*i*r*j/n) for r < n/16, j < 16
+      const auto tw = twiddle_table(n);
+      std::vector<double2> t2((size_t)n);
+      for (int r = 0; r < n / 16; ++r)
+        for (int j = 0; j < 16; ++j) t2[(size_t)r * 16 + j] = tw[(size_t)(r * j) % n];
+      ck(cudaMemcpy(h->tw2, t2.data(), t2.size() * sizeof(double2), cudaMemcpyHostToDevice), "tw2");
+    }
     h->map_state_z = make_field_map(h->state, 6, 2, h->g);
     h->map_work_y = make_field_map(h->work, 12, 1, h->g);
     h->map_work_z = make_field_map(h->work, 12, 2, h->g);

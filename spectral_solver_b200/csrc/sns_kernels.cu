@@ -388,6 +388,290 @@ k_xpass_products(double2* __restrict__ work, const double2* __restrict__ unyq, c
   }
 }
 
+
+// ------------------------------------------------------------------------------------
+// P3 for N = 256 (16 x 16) and N = 512 (16 x 32): two-stage FFTs with one shared-memory
+// round trip each.  Persistent CTAs; the 6 input rows of the next row group arrive by
+// cp.async.bulk into a second staging buffer while the current group is transformed.
+//   inverse stage A : radix 16 over stride-M inputs, the packing Z = U + iV (with the
+//                     mirror and the real-part rule at mx = 0, N/2) fused into the loads
+//   inverse stage B : radix M (M = 32 split over lane pairs, combined by a shuffle);
+//                     z_c = u_c + i*u_shifted_c lands in the (consumed) staging buffer
+//   forward stage A : the products p0 + i*ps fused into the loads, radix 16
+//   forward stage B : radix M, then the r2c unpack P0(k), Ps(k) = (Z(k) +- conj Z(N-k))/2
+//                     with the mirror fetched from the partner lane by a shuffle, and
+//                     128-byte stores straight to HBM
+// The (N/2,0,0) sums of the 12 product planes accumulate in registers per CTA.
+template <int N>
+struct XP {
+  static constexpr int M = N / 16;                 // stage-B radix
+  static constexpr bool PAIR = (M == 32);          // radix 32 as two radix-16 halves + shuffle
+  static constexpr int NH = N / 2;
+  static constexpr int ROWS = (N == 256) ? 2 : 1;  // rows per iteration (192 threads busy)
+  static constexpr int SP = N + N / 16;            // padded sequence (one slot per 16)
+  static constexpr int NT = 192;
+  static constexpr int ROWIN = 6 * (NH + 1);
+  static constexpr int STG = (ROWIN > 3 * SP ? ROWIN : 3 * SP);
+  static constexpr uint32_t kRowBytes = (NH + 1) * sizeof(double2);
+  static constexpr size_t smem = (size_t)(2 * ROWS * STG + ROWS * 6 * SP + N) * sizeof(double2) + 128 +
+                                 2 * sizeof(uint64_t);
+};
+
+__device__ __forceinline__ int pp16(int e) { return e + (e >> 4); }
+
+__device__ __forceinline__ double2 shfl2(double2 v, int src) {
+  return make_double2(__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src));
+}
+__device__ __forceinline__ double2 shfl2_xor(double2 v, int m) {
+  return make_double2(__shfl_xor_sync(0xffffffffu, v.x, m), __shfl_xor_sync(0xffffffffu, v.y, m));
+}
+
+template <int N>
+__global__ void __launch_bounds__(192, 2)
+k_xpass2(double2* __restrict__ work, const double2* __restrict__ unyq, const double2* __restrict__ phase,
+         double scale, int nyq_scalar, double* __restrict__ nyq_part, const double2* __restrict__ tw2_g, Geom g,
+         int* err) {
+  using X = XP<N>;
+  constexpr int M = X::M, NH = X::NH, ROWS = X::ROWS, SP = X::SP, STG = X::STG;
+  extern __shared__ unsigned char smraw[];
+  __shared__ int s_fail;
+  __shared__ double s_nyq[2][12];
+  const uint32_t pad = (128u - (smem_u32(smraw) & 127u)) & 127u;
+  double2* stg = reinterpret_cast<double2*>(smraw + pad);  // [2][ROWS][STG]
+  double2* W = stg + 2 * ROWS * STG;                       // [ROWS][6][SP]
+  double2* tw2 = W + ROWS * 6 * SP;                        // [M][16]: W_N^(r*j)
+  uint64_t* bars = reinterpret_cast<uint64_t*>(tw2 + N);
+  const int tid = threadIdx.x;
+  for (int t = tid; t < N; t += 192) tw2[t] = tw2_g[t];
+  if (tid == 0) {
+    mbar_init(&bars[0], 1);
+    mbar_init(&bars[1], 1);
+    fence_mbar_init();
+    s_fail = 0;
+  }
+  __syncthreads();
+  const long long niter = (long long)N * N / ROWS;
+  auto issue = [&](long long it, int b) {
+    mbar_arrive_expect_tx(&bars[b], ROWS * 6 * X::kRowBytes);
+#pragma unroll
+    for (int r = 0; r < ROWS; ++r) {
+      const long long row = it * ROWS + r;
+#pragma unroll
+      for (int f = 0; f < 6; ++f)
+        bulk_load(stg + (b * ROWS + r) * STG + f * (NH + 1), work + (long long)f * g.field + row * g.pitch,
+                  X::kRowBytes, &bars[b]);
+    }
+  };
+  if (tid == 0) {
+    if (blockIdx.x < niter) issue(blockIdx.x, 0);
+    if (blockIdx.x + gridDim.x < niter) issue(blockIdx.x + gridDim.x, 1);
+  }
+  double nyq_p0 = 0.0, nyq_ps = 0.0;  // owned by the lane that holds k = N/2 of its pair
+  int k = 0;
+  for (long long it = blockIdx.x; it < niter; ++k, it += gridDim.x) {
+    const int b = k & 1;
+    const uint32_t parity = (uint32_t)(k >> 1) & 1u;
+    if (tid == 0 && !mbar_wait_bounded(&bars[b], parity)) s_fail = 1;
+    __syncthreads();
+    if (s_fail) {
+      if (tid == 0) {
+        atomicExch(err, kErrTmaTimeout);
+        (void)mbar_wait_bounded(&bars[b ^ 1], (uint32_t)((k + 1) >> 1) & 1u);
+      }
+      return;
+    }
+    (void)mbar_try_wait(&bars[b], parity);
+    double2* S = stg + b * ROWS * STG;
+
+    // ---- inverse stage A: (r, c, t), packing fused into the loads
+    if (tid < ROWS * 3 * M) {
+      const int t = tid % M, c = (tid / M) % 3, r = tid / (3 * M);
+      const double2* Ur = S + r * STG + (2 * c) * (NH + 1);
+      const double2* Vr = Ur + (NH + 1);
+      double2 v[16];
+#pragma unroll
+      for (int q = 0; q < 16; ++q) {
+        const int x = t + M * q;
+        double2 z;
+        if (x == 0) {
+          z = make_double2(Ur[0].x, Vr[0].x);
+        } else if (x < NH) {
+          const double2 U = Ur[x], V = Vr[x];
+          z = make_double2(U.x - V.y, U.y + V.x);
+        } else if (x == NH) {
+          double2 U, V;
+          if (nyq_scalar) {
+            U = cscale(unyq[(long long)c * g.field + NH], scale);
+            V = cmul(U, phase[NH + 3 * N / 2]);
+          } else {
+            U = Ur[NH];
+            V = Vr[NH];
+          }
+          z = make_double2(U.x, V.x);
+        } else {
+          const double2 U = Ur[N - x], V = Vr[N - x];
+          z = make_double2(U.x + V.y, V.x - U.y);
+        }
+        v[q] = z;
+      }
+      dft16<+1>(v);
+      double2* Wc = W + (r * 6 + c) * SP;
+#pragma unroll
+      for (int q = 0; q < 16; ++q) Wc[pp16(16 * t + q)] = v[q];
+    }
+    __syncthreads();
+
+    // ---- inverse stage B: z_c into the staging buffer (its inputs are consumed)
+    if constexpr (X::PAIR) {
+      if (tid < 96) {
+        const int lane = tid & 31, c = tid >> 5, j = lane & 15, h = lane >> 4;
+        const double2* Wc = W + c * SP;
+        double2 v[16];
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+          const int rr = 2 * i + h;
+          v[i] = cmulc(Wc[pp16(j + 16 * rr)], tw2[rr * 16 + j]);  // inverse twiddle = conj
+        }
+        dft16<+1>(v);
+        if (h) {
+#pragma unroll
+          for (int q = 1; q < 16; ++q) v[q] = cmulc(v[q], tw2[16 * 16 + q]);  // conj W32^q
+        }
+        double2* Zc = S + c * SP;
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+          const double2 o = shfl2_xor(v[q], 16);
+          const double2 z = h ? csub(o, v[q]) : cadd(v[q], o);
+          Zc[pp16(j + 16 * (q + 16 * h))] = z;
+        }
+      }
+    } else {
+      if (tid < ROWS * 3 * 16) {
+        const int j = tid & 15, c = (tid >> 4) % 3, r = tid / 48;
+        const double2* Wc = W + (r * 6 + c) * SP;
+        double2 v[16];
+#pragma unroll
+        for (int q = 0; q < 16; ++q) v[q] = q == 0 ? Wc[pp16(j)] : cmulc(Wc[pp16(j + 16 * q)], tw2[q * 16 + j]);
+        dft16<+1>(v);
+        double2* Zc = S + r * STG + c * SP;
+#pragma unroll
+        for (int q = 0; q < 16; ++q) Zc[pp16(j + 16 * q)] = v[q];
+      }
+    }
+    __syncthreads();
+
+    // ---- forward stage A: products fused into the loads
+    {
+      const int t = tid % M, ab = (tid / M) % 6, r = tid / (6 * M);
+      // pairs 00 01 02 11 12 22
+      const int ca = (ab >= 3) + (ab >= 5), cb = ab < 3 ? ab : (ab < 5 ? ab - 2 : 2);
+      const double2* Za = S + r * STG + ca * SP;
+      const double2* Zb = S + r * STG + cb * SP;
+      double2 v[16];
+#pragma unroll
+      for (int q = 0; q < 16; ++q) {
+        const int x = pp16(t + M * q);
+        const double2 za = Za[x], zb = Zb[x];
+        v[q] = make_double2(za.x * zb.x, za.y * zb.y);
+      }
+      dft16<-1>(v);
+      double2* Wp = W + (r * 6 + ab) * SP;
+#pragma unroll
+      for (int q = 0; q < 16; ++q) Wp[pp16(16 * t + q)] = v[q];
+    }
+    __syncthreads();
+
+    // ---- forward stage B, r2c unpack through the partner lane, stores to HBM
+    if constexpr (X::PAIR) {
+      const int lane = tid & 31, ab = tid >> 5, j = lane & 15, h = lane >> 4;
+      const double2* Wp = W + ab * SP;
+      double2 v[16];
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        const int rr = 2 * i + h;
+        v[i] = cmul(Wp[pp16(j + 16 * rr)], tw2[rr * 16 + j]);
+      }
+      dft16<-1>(v);
+      if (h) {
+#pragma unroll
+        for (int q = 1; q < 16; ++q) v[q] = cmul(v[q], tw2[16 * 16 + q]);
+      }
+#pragma unroll
+      for (int q = 0; q < 16; ++q) {
+        const double2 o = shfl2_xor(v[q], 16);
+        v[q] = h ? csub(o, v[q]) : cadd(v[q], o);  // X(j + 16 (q + 16 h))
+      }
+      const int partner = ((16 - j) & 15) + 16 * (1 - h);
+      const long long row = it;
+      double2* o0 = work + (long long)(2 * ab) * g.field + row * g.pitch;
+      double2* o1 = o0 + g.field;
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        const double2 send = j == 0 ? v[(16 - i) & 15] : v[15 - i];
+        const double2 recv = shfl2(send, partner);
+        const double2 zm = (j == 0 && i == 0) ? v[0] : recv;
+        const int kk = j + 16 * (16 * h + i);
+        if (kk <= NH) {
+          double2 A, B;
+          unpack_pair(v[i], zm, &A, &B);
+          o0[kk] = A;
+          o1[kk] = B;
+          if (kk == NH) {
+            nyq_p0 += A.x;
+            nyq_ps += B.x;
+          }
+        }
+      }
+    } else {
+      const int j = tid & 15, sq = tid >> 4, r = sq / 6, ab = sq % 6;
+      const double2* Wp = W + (r * 6 + ab) * SP;
+      double2 v[16];
+#pragma unroll
+      for (int q = 0; q < 16; ++q) v[q] = q == 0 ? Wp[pp16(j)] : cmul(Wp[pp16(j + 16 * q)], tw2[q * 16 + j]);
+      dft16<-1>(v);
+      const int lane = tid & 31;
+      const int partner = (lane & 16) + ((16 - j) & 15);
+      const long long row = it * ROWS + r;
+      double2* o0 = work + (long long)(2 * ab) * g.field + row * g.pitch;
+      double2* o1 = o0 + g.field;
+#pragma unroll
+      for (int q = 0; q < 16; ++q) {
+        const double2 recv = shfl2(v[15 - q], partner);
+        const double2 zm = j == 0 ? v[(16 - q) & 15] : recv;
+        const int kk = j + 16 * q;
+        if (kk <= NH) {
+          double2 A, B;
+          unpack_pair(v[q], zm, &A, &B);
+          o0[kk] = A;
+          o1[kk] = B;
+          if (kk == NH) {
+            nyq_p0 += A.x;
+            nyq_ps += B.x;
+          }
+        }
+      }
+    }
+    __syncthreads();
+    if (tid == 0 && it + 2LL * gridDim.x < niter) issue(it + 2LL * gridDim.x, b);
+  }
+  // per-CTA Nyquist partials, fixed order: [field][cta]
+  if constexpr (X::PAIR) {
+    const int lane = tid & 31, ab = tid >> 5;
+    if (lane == 16) {  // j = 0, h = 1 holds k = N/2
+      nyq_part[(2 * ab) * gridDim.x + blockIdx.x] = nyq_p0;
+      nyq_part[(2 * ab + 1) * gridDim.x + blockIdx.x] = nyq_ps;
+    }
+  } else {
+    const int j = tid & 15, sq = tid >> 4, r = sq / 6, ab = sq % 6;
+    if (j == 0) {
+      s_nyq[r][2 * ab] = nyq_p0;
+      s_nyq[r][2 * ab + 1] = nyq_ps;
+    }
+    __syncthreads();
+    if (tid < 12) nyq_part[tid * gridDim.x + blockIdx.x] = s_nyq[0][tid] + s_nyq[1][tid];
+  }
+}
+
 // Nyquist-plane sums: column N/2 of each of the 12 product fields summed over all rows
 // (the (N/2,0,0) output of the y/z forward transforms is the plain sum of the plane).
 // grid 12, fixed summation order.
@@ -420,6 +704,18 @@ __device__ __forceinline__ double2 minus_i_k(double2 a, int k) {
   return make_double2(rk * a.y, -rk * a.x);
 }
 
+// Dealiased product value of one pair at one mode (accumulate lambda, :928-931).
+__device__ __forceinline__ double2 pair_value(double2 p0, double2 ps, double2 phase, bool keep, int dealias) {
+  double2 value = dealias ? cscale(cadd(p0, cmulc(ps, phase)), 0.5) : p0;
+  if (!keep) value = make_double2(0.0, 0.0);
+  return value;
+}
+
+// Viscous term, Leray projection and mask (:955-974), then the RK stage update and the
+// projection of u (:994-1039) -- or the RHS itself in modes 1 and 2.
+__device__ __forceinline__ void finish_mode(double2 r[3], int ix, int iy, int iz, int n, double2 uu[3], double2 gg[3],
+                                            bool load_g, double2 rr[3], const SweepArgs& a);
+
 __device__ __forceinline__ void sweep_mode(const ModeIn& in, int ix, int iy, int iz, int n, double2 phase,
                                            double2 uu[3], double2 gg[3], bool load_g, double2 rr[3],
                                            const SweepArgs& a) {
@@ -431,13 +727,17 @@ __device__ __forceinline__ void sweep_mode(const ModeIn& in, int ix, int iy, int
   const int pb[6] = {0, 1, 2, 1, 2, 2};
 #pragma unroll
   for (int p = 0; p < 6; ++p) {
-    double2 value;
-    if (a.dealias) value = cscale(cadd(in.p0[p], cmulc(in.ps[p], phase)), 0.5);
-    else value = in.p0[p];
-    if (!keep) value = make_double2(0.0, 0.0);
+    const double2 value = pair_value(in.p0[p], in.ps[p], phase, keep, a.dealias);
     r[pa[p]] = cadd(r[pa[p]], minus_i_k(value, kv[pb[p]]));
     if (pa[p] != pb[p]) r[pb[p]] = cadd(r[pb[p]], minus_i_k(value, kv[pa[p]]));
   }
+  finish_mode(r, ix, iy, iz, n, uu, gg, load_g, rr, a);
+}
+
+__device__ __forceinline__ void finish_mode(double2 r[3], int ix, int iy, int iz, int n, double2 uu[3], double2 gg[3],
+                                            bool load_g, double2 rr[3], const SweepArgs& a) {
+  const int m2 = ix * ix + iy * iy + iz * iz;
+  const bool keep = 4LL * m2 <= (long long)n * n;
   const double k2 = (double)m2;
   if (a.mode == 2) {  // nonlinear term only: masked, neither viscous term nor projection
     rr[0] = r[0];
@@ -481,7 +781,7 @@ __device__ __forceinline__ void sweep_mode(const ModeIn& in, int ix, int iy, int
 template <int N>
 __global__ void __launch_bounds__(256)
 k_sweep(const double2* __restrict__ work, double2* __restrict__ u, double2* __restrict__ gbuf,
-        double2* __restrict__ rhs, const double* __restrict__ nyqsum, const double2* __restrict__ phase,
+        double2* __restrict__ rhs, const double* __restrict__ nyq_part, int nparts, const double2* __restrict__ phase,
         SweepArgs a, Geom g) {
   constexpr int NH = N / 2;
   const long long e = (long long)blockIdx.x * 256 + threadIdx.x;
@@ -532,13 +832,24 @@ k_sweep(const double2* __restrict__ work, double2* __restrict__ u, double2* __re
       }
     }
   }
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
-    // the self-conjugate Nyquist mode (N/2, 0, 0), column nh of row (0, 0)
+  if (blockIdx.x == 0 && threadIdx.x < 32) {
+    // the self-conjugate Nyquist mode (N/2, 0, 0), column nh of row (0, 0): warp 0 sums
+    // the per-CTA plane sums (lane-strided, then a fixed shuffle tree: deterministic)
+    double part[12];
+#pragma unroll
+    for (int f = 0; f < 12; ++f) {
+      double acc = 0.0;
+      for (int i = threadIdx.x; i < nparts; i += 32) acc += nyq_part[f * nparts + i];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+      part[f] = acc;
+    }
+  if (threadIdx.x == 0) {
     ModeIn in;
 #pragma unroll
     for (int p = 0; p < 6; ++p) {
-      in.p0[p] = make_double2(nyqsum[2 * p], 0.0);
-      in.ps[p] = make_double2(nyqsum[2 * p + 1], 0.0);
+      in.p0[p] = make_double2(part[2 * p], 0.0);
+      in.ps[p] = make_double2(part[2 * p + 1], 0.0);
     }
     const long long idx = NH;
     double2 uu[3], gg[3], rr[3];
@@ -559,6 +870,243 @@ k_sweep(const double2* __restrict__ work, double2* __restrict__ u, double2* __re
       }
     }
   }
+  }
+}
+
+
+
+// The self-conjugate mode (N/2, 0, 0) for the fused P5 path: one warp sums the x pass's
+// per-CTA plane sums in a fixed order and runs the sweep on that single mode (column N/2
+// of row 0, which no P5 tile touches).
+template <int N>
+__global__ void __launch_bounds__(32) k_nyq_mode(double2* __restrict__ u, double2* __restrict__ gbuf,
+                                                 double2* __restrict__ rhs, const double* __restrict__ nyq_part,
+                                                 int nparts, const double2* __restrict__ phase, SweepArgs a, Geom g) {
+  constexpr int NH = N / 2;
+  const int tid = threadIdx.x;
+  const bool load_g = a.stage > 0;
+  double part[12];
+#pragma unroll
+  for (int f = 0; f < 12; ++f) {
+    double acc = 0.0;
+    for (int i = tid; i < nparts; i += 32) acc += nyq_part[f * nparts + i];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    part[f] = acc;
+  }
+  if (tid != 0) return;
+  ModeIn in;
+#pragma unroll
+  for (int p = 0; p < 6; ++p) {
+    in.p0[p] = make_double2(part[2 * p], 0.0);
+    in.ps[p] = make_double2(part[2 * p + 1], 0.0);
+  }
+  double2 uu[3], gg[3], rr[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    uu[c] = u[(long long)c * g.field + NH];
+    gg[c] = load_g ? gbuf[(long long)c * g.field + NH] : make_double2(0, 0);
+  }
+  sweep_mode(in, NH, 0, 0, N, phase[NH + 3 * N / 2], uu, gg, load_g, rr, a);
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    if (a.mode != 0) {
+      rhs[(long long)c * g.field + NH] = rr[c];
+    } else {
+      u[(long long)c * g.field + NH] = uu[c];
+      gbuf[(long long)c * g.field + NH] = gg[c];
+    }
+  }
+}
+
+// ------------------------------------------------------------------------------------
+// P5 fused (N = 128, 256, 512): forward z pass of the 12 product fields and the whole
+// k-space sweep in one persistent kernel, so the transformed products never return to HBM.
+// A tile is (8 columns mx, one my, all mz); its 12 field tiles arrive one after another
+// through TMA (double-buffered).  The z FFT leaves each thread 8 modes in registers:
+//   P0 field of pair p -> parked in tensor memory;
+//   Ps field of pair p -> combined with the parked P0 into the dealiased value, whose -i k
+//                          contributions accumulate into r_x, r_y, r_z in tensor memory, in
+//                          the reference's order (pairs 00 01 02 11 12 22);
+//   after the 12th      -> viscous term, Leray projection, RK3 update and projection of u.
+// Tensor memory per thread: 4 x 32 columns (P0, r_x, r_y, r_z: 8 complex each).
+template <int N>
+constexpr uint32_t p5_cols() { return N == 512 ? 512u : (N == 256 ? 256u : 128u); }
+template <int N>
+constexpr int nt_p5() { return nt_tma<N>(); }
+
+template <int N>
+__global__ void __launch_bounds__(nt_p5<N>(), tma_minb<N>())
+k_p5(const __grid_constant__ CUtensorMap map, double2* __restrict__ u, double2* __restrict__ gbuf,
+     double2* __restrict__ rhs, const double* __restrict__ nyq_part, int nparts, const double2* __restrict__ tw,
+     const double2* __restrict__ phase, SweepArgs a, int ncb, Geom g, int* err) {
+  constexpr int NT = nt_p5<N>();
+  constexpr int BR = box_rows<N>();
+  constexpr int NBOX = N / BR;
+  constexpr int NH = N / 2;
+  constexpr uint32_t kTileBytes = 8u * N * sizeof(double2);
+  constexpr uint32_t COLS = p5_cols<N>();
+  using RO = RegOut<N, NT>;
+  constexpr int MPT = RO::KB * RO::R;  // modes per thread
+  constexpr int CW = 4 * MPT;          // tensor-memory words per field of modes
+  static_assert(RO::R == 4 || RO::R == 8, "last radix moves through tensor memory");
+  static_assert((NT / 32 + 3) / 4 * 4 * CW <= (int)COLS, "tensor memory budget");
+  static_assert((8 * (N / RO::R)) % NT == 0, "every thread owns whole butterflies");
+  extern __shared__ unsigned char smraw[];
+  __shared__ int s_fail;
+  __shared__ uint32_t s_tmem;
+  const uint32_t pad = (128u - (smem_u32(smraw) & 127u)) & 127u;
+  double2* in0 = reinterpret_cast<double2*>(smraw + pad);
+  double2* in1 = in0 + 8 * N;
+  double2* W = in1 + 8 * N;
+  double2* s_tw = W + 8 * N;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(s_tw + N);
+  const int tid = threadIdx.x, warp = tid >> 5;
+  for (int t = tid; t < N; t += NT) s_tw[t] = tw[t];
+  if (tid == 0) {
+    mbar_init(&bars[0], 1);
+    mbar_init(&bars[1], 1);
+    fence_mbar_init();
+    s_fail = 0;
+  }
+  if (warp == 0) {
+    tmem_alloc(&s_tmem, COLS);
+    tmem_relinquish();
+  }
+  __syncthreads();
+  const uint32_t tbase = s_tmem;
+  // this thread's lane and columns: P0 park [0, CW), r_x, r_y, r_z at CW * (1 + c)
+  const uint32_t tq = tbase + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)((warp >> 2) * 4 * CW);
+  const bool load_g = a.stage > 0;
+
+  const long long ntiles = (long long)ncb * N;  // (cb, my)
+  const long long mytiles = blockIdx.x < ntiles ? (ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+  const long long nunits = 12 * mytiles;
+  auto issue = [&](long long ul, int b) {
+    const long long t = blockIdx.x + (ul / 12) * gridDim.x;
+    const int f = (int)(ul % 12);
+    const int cb = (int)(t % ncb), my = (int)(t / ncb);
+    double2* dst = b ? in1 : in0;
+    mbar_arrive_expect_tx(&bars[b], kTileBytes);
+#pragma unroll
+    for (int k = 0; k < NBOX; ++k) tma_load_4d(dst + k * BR * 8, &map, &bars[b], cb * 16, my, k * BR, f);
+  };
+  if (tid == 0) {
+    if (nunits > 0) issue(0, 0);
+    if (nunits > 1) issue(1, 1);
+  }
+  for (long long ul = 0; ul < nunits; ++ul) {
+    const int b = (int)(ul & 1);
+    const uint32_t parity = (uint32_t)(ul >> 1) & 1u;
+    if (tid == 0 && !mbar_wait_bounded(&bars[b], parity)) s_fail = 1;
+    __syncthreads();
+    if (s_fail) {
+      if (tid == 0) {
+        atomicExch(err, kErrTmaTimeout);
+        (void)mbar_wait_bounded(&bars[b ^ 1], (uint32_t)((ul + 1) >> 1) & 1u);
+      }
+      if (warp == 0) tmem_dealloc(tbase, COLS);
+      return;
+    }
+    (void)mbar_try_wait(&bars[b], parity);
+    const double2* IN = b ? in1 : in0;
+    const long long t = blockIdx.x + (ul / 12) * gridDim.x;
+    const int f = (int)(ul % 12);
+    const int cb = (int)(t % ncb), my = (int)(t / ncb);
+    const int mx0 = cb * 8;
+    // Each radix butterfly of the last stage hands its R modes to the sink: column
+    // s = b & 7 (b = tid + i*NT), z index (j/NS)*NS*R + j%NS + r*NS with j = b >> 3; mode
+    // q = i*R + r of this thread owns tensor-memory columns [4q, 4q + 4) of every block.
+    const int iy = signed_mode(my, N);
+    const int p = f >> 1;
+    const int ca = (p >= 3) + (p >= 5), cbp = p < 3 ? p : (p < 5 ? p - 2 : 2);
+    auto sink = [&](int i, double2* v) {
+      constexpr int R = RO::R, NS = RO::NS;
+      const int bb = tid + i * NT, s_ = bb & 7, j = bb >> 3;
+      const uint32_t col = (uint32_t)(4 * R * i);
+      if ((f & 1) == 0) {
+        tmem_st<R>(tq + col, v);  // park P0 of this pair
+        return;
+      }
+      const int ix = mx0 + s_;
+      int izs[R];
+      {
+        double2 p0[R];
+        tmem_ld<R>(tq + col, p0);
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          izs[r] = signed_mode((j / NS) * NS * R + (j % NS) + r * NS, N);
+          const bool keep = 4LL * (ix * ix + iy * iy + izs[r] * izs[r]) <= (long long)N * N;
+          v[r] = pair_value(p0[r], v[r], __ldg(&phase[ix + iy + izs[r] + 3 * N / 2]), keep, a.dealias);
+        }
+      }
+      // r_a += -i k_b value; r_b += -i k_a value (a != b); the first touch starts the sum
+#pragma unroll
+      for (int side = 0; side < 2; ++side) {
+        if (side == 1 && ca == cbp) break;
+        const int dst = side == 0 ? ca : cbp, kc = side == 0 ? cbp : ca;
+        const bool first = side == 0 ? (p == 0) : (p == 1 || p == 2);  // r_x at 00, r_y at 01, r_z at 02
+        const uint32_t ta = tq + (uint32_t)(CW * (1 + dst)) + col;
+        double2 r[R];
+        if (!first) tmem_ld<R>(ta, r);
+#pragma unroll
+        for (int rr = 0; rr < R; ++rr) {
+          const int kk = kc == 0 ? ix : (kc == 1 ? iy : izs[rr]);
+          const double2 c = minus_i_k(v[rr], kk);
+          r[rr] = first ? c : cadd(r[rr], c);
+        }
+        tmem_st<R>(ta, r);
+      }
+    };
+    tile_fft_sink<N, -1, NT>([&](int s_, int e_) { return IN[e_ * 8 + s_]; }, W, s_tw, tid, sink);
+    tmem_wait_st();
+    __syncthreads();  // IN[b] and W are free again
+    if (tid == 0 && ul + 2 < nunits) issue(ul + 2, b);
+    auto mode_s = [&](int q) { return (tid + (q / RO::R) * NT) & 7; };
+    auto mode_e = [&](int q) {
+      const int j = (tid + (q / RO::R) * NT) >> 3, r = q % RO::R;
+      return (j / RO::NS) * RO::NS * RO::R + (j % RO::NS) + r * RO::NS;
+    };
+    if (f == 11) {
+#pragma unroll 1
+      for (int q = 0; q < MPT; ++q) {
+        double2 r3[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) r3[c] = tmem_ld1(tq + CW * (1 + c) + 4 * q);
+        const int ix = mx0 + mode_s(q);
+        if (ix >= NH) continue;
+        const int ez = mode_e(q);
+        const int iz = signed_mode(ez, N);
+        const long long row = (long long)ez * N + my;
+        const long long idx = row * g.pitch + ix;
+        double2 uu[3], gg[3], rr[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          uu[c] = u[(long long)c * g.field + idx];
+          gg[c] = load_g ? gbuf[(long long)c * g.field + idx] : make_double2(0, 0);
+        }
+        finish_mode(r3, ix, iy, iz, N, uu, gg, load_g, rr, a);
+        const bool nyq_zero = ix == 0 && row != 0;  // plane mx = N/2 is zero off (N/2,0,0)
+        const long long inq = row * g.pitch + NH;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          if (a.mode != 0) {
+            rhs[(long long)c * g.field + idx] = rr[c];
+            if (nyq_zero) rhs[(long long)c * g.field + inq] = make_double2(0.0, 0.0);
+          } else {
+            u[(long long)c * g.field + idx] = uu[c];
+            gbuf[(long long)c * g.field + idx] = gg[c];
+            if (nyq_zero) {
+              u[(long long)c * g.field + inq] = make_double2(0.0, 0.0);
+              gbuf[(long long)c * g.field + inq] = make_double2(0.0, 0.0);
+            }
+          }
+        }
+      }
+    }
+  }
+  __syncthreads();
+  if (warp == 0) tmem_dealloc(tbase, COLS);
 }
 
 // ------------------------------------------------------------------------------------
@@ -903,10 +1451,52 @@ struct Launch {
   static void nyq_reduce(const double2* work, double* sums, Geom g, cudaStream_t st) {
     k_nyq_reduce<<<12, 256, 0, st>>>(work, sums, g);
   }
-  static void sweep(const double2* work, double2* u, double2* gbuf, double2* rhs, const double* nyqsum,
+  static void sweep(const double2* work, double2* u, double2* gbuf, double2* rhs, const double* nyq_part, int nparts,
                     const double2* phase, SweepArgs a, Geom g, cudaStream_t st) {
     const long long total = (long long)N * N * (N / 2);
-    k_sweep<N><<<(unsigned)((total + 255) / 256), 256, 0, st>>>(work, u, gbuf, rhs, nyqsum, phase, a, g);
+    k_sweep<N><<<(unsigned)((total + 255) / 256), 256, 0, st>>>(work, u, gbuf, rhs, nyq_part, nparts, phase, a, g);
+  }
+  static void xpass2(double2* work, const double2* unyq, const double2* phase, double scale, int nyq_scalar,
+                     double* nyq_part, const double2* tw2, Geom g, int grid, int* err, cudaStream_t st) {
+    if constexpr (N == 256 || N == 512) {
+      k_xpass2<N><<<grid, XP<N>::NT, XP<N>::smem, st>>>(work, unyq, phase, scale, nyq_scalar, nyq_part, tw2, g, err);
+    }
+  }
+  static void p5(const CUtensorMap& map, double2* u, double2* gbuf, double2* rhs, const double* nyq_part, int nparts,
+                 const double2* tw, const double2* phase, SweepArgs a, int ncb, Geom g, int grid, int* err,
+                 cudaStream_t st) {
+    if constexpr (N == 128 || N == 256 || N == 512) {
+      k_nyq_mode<N><<<1, 32, 0, st>>>(u, gbuf, rhs, nyq_part, nparts, phase, a, g);
+      k_p5<N><<<grid, nt_p5<N>(), tma_smem<N>(), st>>>(map, u, gbuf, rhs, nyq_part, nparts, tw, phase, a, ncb, g,
+                                                        err);
+    }
+  }
+  // Persistent grid of the fused P5 (0: this size runs forward z + sweep as two kernels).
+  static int p5_grid(int nsm) {
+    if constexpr (N == 128 || N == 256 || N == 512) {
+      int nb = 0;
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_p5<N>, nt_p5<N>(), tma_smem<N>());
+      // tensor memory holds at most 512 columns per SM
+      const int cap = 512 / (int)p5_cols<N>();
+      nb = nb < 1 ? 1 : (nb > cap ? cap : nb);
+      return nsm * nb;
+    } else {
+      (void)nsm;
+      return 0;
+    }
+  }
+  // Persistent grid of the two-stage x pass (0: this size uses the generic x pass).
+  static int xpass2_grid(int nsm) {
+    if constexpr (N == 256 || N == 512) {
+      int nb = 0;
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_xpass2<N>, XP<N>::NT, XP<N>::smem);
+      const long long niter = (long long)N * N / XP<N>::ROWS;
+      long long grid = (long long)nsm * (nb > 0 ? nb : 1);
+      return (int)(grid < niter ? grid : niter);
+    } else {
+      (void)nsm;
+      return 0;
+    }
   }
   static void xpass_r2c(const double* in, double2* out, int nf, const double2* tw, Geom g, cudaStream_t st) {
     k_xpass_r2c<N><<<dim3(N * N / 2, nf), nt_x<N>(), x_smem(1), st>>>(in, out, tw, g);
@@ -948,6 +1538,8 @@ struct Launch {
   }
   // Opt every kernel of this size into its dynamic shared memory (once per process).
   static void init() {
+    if constexpr (N == 256 || N == 512) set_smem(k_xpass2<N>, XP<N>::smem);
+    if constexpr (N == 128 || N == 256 || N == 512) set_smem(k_p5<N>, tma_smem<N>());
     set_smem(k_yz_tma<N, 2, +1, 1>, tma_smem<N>());
     set_smem(k_yz_tma<N, 1, -1, 0>, tma_smem<N>());
     set_smem(k_yz_tma<N, 1, +1, 0>, tma_smem<N>());
@@ -965,7 +1557,8 @@ struct Launch {
   }
   static const Ops* table() {
     static const Ops ops = {N, init, zpass_inv_phase, ypass, zpass, xpass_products, nyq_reduce, sweep,
-                            xpass_r2c, xpass_c2r, xpass_diag, yz_tma, tma_blocks_per_sm};
+                            xpass_r2c, xpass_c2r, xpass_diag, yz_tma, tma_blocks_per_sm, xpass2, xpass2_grid,
+                            p5, p5_grid};
     return &ops;
   }
 };

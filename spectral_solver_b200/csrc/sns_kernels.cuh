@@ -59,8 +59,9 @@ struct Ops {
                          int nyq_scalar, double* partials, const double2* tw, Geom g, cudaStream_t st);
   // Nyquist-plane sums of the 12 product fields (column nh, summed over rows)
   void (*nyq_reduce)(const double2* work, double* sums, Geom g, cudaStream_t st);
-  // fused k-space sweep; rhs may be null in RK mode
-  void (*sweep)(const double2* work, double2* u, double2* gbuf, double2* rhs, const double* nyqsum,
+  // fused k-space sweep; rhs may be null in RK mode; the (N/2,0,0) product values are the
+  // fixed-order sums of nparts partials per field ([field][nparts])
+  void (*sweep)(const double2* work, double2* u, double2* gbuf, double2* rhs, const double* nyq_part, int nparts,
                 const double2* phase, SweepArgs a, Geom g, cudaStream_t st);
   // generic real rows -> half rows (x r2c), nf fields of real data with row pitch n doubles
   void (*xpass_r2c)(const double* in, double2* out, int nf, const double2* tw, Geom g, cudaStream_t st);
@@ -73,6 +74,15 @@ struct Ops {
   void (*yz_tma)(const CUtensorMap& map, int axis, int dir, int variant, TmaArgs a, const double2* tw,
                  const double2* phase, Geom g, int grid, cudaStream_t st);
   int (*tma_blocks_per_sm)();
+  // two-stage persistent x pass (N = 256, 512); writes [12][grid] Nyquist partials
+  void (*xpass2)(double2* work, const double2* unyq, const double2* phase, double scale, int nyq_scalar,
+                 double* nyq_part, const double2* tw2, Geom g, int grid, int* err, cudaStream_t st);
+  int (*xpass2_grid)(int nsm);
+  // fused forward z pass + k-space sweep (N = 128, 256, 512), TMA-fed, accumulators in TMEM
+  void (*p5)(const CUtensorMap& map, double2* u, double2* gbuf, double2* rhs, const double* nyq_part, int nparts,
+             const double2* tw, const double2* phase, SweepArgs a, int ncb, Geom g, int grid, int* err,
+             cudaStream_t st);
+  int (*p5_grid)(int nsm);
 };
 
 const Ops* ops_for(int n);  // nullptr when the size has no FFT plan

@@ -128,3 +128,18 @@ def test_seeded_trajectory_128_100_steps():
             for key in ("kinetic_energy", "dissipation"):
                 worst = max(worst, rel(d[key], dr[key]))
     assert worst <= 1e-10, worst
+
+
+def test_rhs_512_seeded():
+    """The 512^3 pass variants (radix-32 split over lane pairs in the x pass, two TMA
+    boxes per tile in the y/z passes) against the oracle: one RHS, 1e-12 relative L2."""
+    from spectral_solver_b200 import Solver
+    n = 512
+    o = seeded_oracle(n, seed=3, amp=1e-2, kmax=16)
+    with Solver(n, 1600.0, seed=3, pert_amp=1e-2, pert_kmax=16) as s:
+        u = s.get_state()
+        assert rel_l2(u, [half_to_full(c) for c in o.u_hat]) < 1e-13
+        r = s.rhs(u)
+    del u
+    r_ref = [half_to_full(c) for c in o.compute_rhs()]
+    assert rel_l2(r, r_ref) < 1e-12
