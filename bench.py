@@ -34,10 +34,19 @@ RE = 1600.0
 DT = 1e-3
 
 # Algorithmic bytes per launch of each pass, in units of S = N^3 * 8 B (one FP64 real field
-# or one half-spectrum complex field): every field read or written once.
-PASS_BYTES_S = {"zpass_inv_phase": 9, "ypass_inv": 12, "xpass_products": 18, "nyq_reduce": 0,
-                "ypass_fwd": 24, "zpass_fwd": 24, "sweep": 23}
-LAUNCHES_PER_STEP = 3 * 7
+# or one half-spectrum complex field): every field read or written once.  At N = 128, 256,
+# 512 the forward z pass and the sweep are one fused kernel ("p5_sweep": 12 product fields
+# + u + g in, u + g out; g is not read in the first stage, hence 23 on average).
+PASS_BYTES_S = {"p1_zinv_phase": 9, "p2_yinv": 12, "p3_xpass": 18, "p3_nyq": 0,
+                "p4_yfwd": 24, "p5_zfwd": 24, "p5_sweep": 23}
+# kernels per RK3 stage at N = 512: P1, P2, P3, P4, the (N/2,0,0) mode, fused P5
+LAUNCHES_PER_STEP = 3 * 6
+# DRAM traffic per launch per grid point (dram__bytes_read.sum + dram__bytes_write.sum) from
+# single-launch ncu captures at 256^3 (profiles/k_*_256_fp64.txt), scaled by N^3: traffic
+# grows with the grid points, and the 512^3 workload is too large for a full capture.
+TRAFFIC_PER_POINT = {"p5_sweep": 3.262e9 / 256 ** 3, "p3_xpass": 2.445e9 / 256 ** 3,
+                     "p4_yfwd": 3.268e9 / 256 ** 3, "p1_zinv_phase": 1.166e9 / 256 ** 3,
+                     "p2_yinv": 1.582e9 / 256 ** 3}
 
 
 def load_peaks():
@@ -265,7 +274,9 @@ def run_b200(args, world, rank, local, pg):
             "clocks": clocks,
             "gpu_launches": LAUNCHES_PER_STEP * args.steps,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None, "kernel": top,
+                         "frac": achieved / peak,
+                         "traffic": (TRAFFIC_PER_POINT[top] * n ** 3) if top in TRAFFIC_PER_POINT else None,
+                         "kernel": top,
                          "peak_source": f"hbm_gbs {peak_kind}",
                          "algorithmic_bytes_per_launch": PASS_BYTES_S[top] * S,
                          "mean_launch_ms": prof[top]},

@@ -106,6 +106,10 @@ int sns_dump_velocity(sns_handle* h, double* const phys[3]);
  * own viscosity to the backend's handle). */
 int sns_set_viscosity(sns_handle* h, double nu);
 
+/* Persistent grids chosen at creation: out[0] TMA y/z passes, out[1] two-stage x pass
+ * (0 = generic), out[2] fused forward-z + sweep (0 = two kernels), out[3] SM count. */
+int sns_launch_config(const sns_handle* h, int* out, int count);
+
 /* Grid size and device bytes held by the handle. */
 int sns_grid_size(const sns_handle* h);
 size_t sns_device_bytes(const sns_handle* h);

@@ -56,6 +56,7 @@ SIGNATURES = {
     "sns_max_velocity": (C.c_int, [_H, _DP]),
     "sns_dump_velocity": (C.c_int, [_H, _DPP]),
     "sns_set_viscosity": (C.c_int, [_H, C.c_double]),
+    "sns_launch_config": (C.c_int, [_H, C.POINTER(C.c_int), C.c_int]),
     "sns_grid_size": (C.c_int, [_H]),
     "sns_device_bytes": (C.c_size_t, [_H]),
     "sns_time_steps": (C.c_int, [_H, C.c_double, C.c_int, _DP]),
@@ -63,7 +64,7 @@ SIGNATURES = {
     "sns_profile_passes": (C.c_int, [_H, C.c_double, C.c_int, _DP]),
 }
 
-PASS_NAMES = ("zpass_inv_phase", "ypass_inv", "xpass_products", "nyq_reduce", "ypass_fwd", "zpass_fwd", "sweep")
+PASS_NAMES = ("p1_zinv_phase", "p2_yinv", "p3_xpass", "p3_nyq", "p4_yfwd", "p5_zfwd", "p5_sweep")
 
 _lib = None
 
@@ -213,6 +214,11 @@ class Solver:
         out = (C.c_double * len(PASS_NAMES))()
         self._check(self.lib.sns_profile_passes(self.h, dt, nsteps, out))
         return dict(zip(PASS_NAMES, list(out)))
+
+    def launch_config(self) -> dict:
+        out = (C.c_int * 4)()
+        self._check(self.lib.sns_launch_config(self.h, out, 4))
+        return dict(tma_grid=out[0], xpass_grid=out[1], p5_grid=out[2], sms=out[3])
 
     def device_bytes(self) -> int:
         return int(self.lib.sns_device_bytes(self.h))

@@ -577,6 +577,17 @@ int sns_set_viscosity(sns_handle* h, double nu) {
   return SNS_OK;
 }
 
+int sns_launch_config(const sns_handle* h, int* out, int count) {
+  if (h == nullptr || out == nullptr || count < 4) return SNS_ERR_INVALID;
+  out[0] = h->tma_grid;
+  out[1] = h->x2_grid;
+  out[2] = h->p5_grid;
+  int nb = 0;
+  cudaDeviceGetAttribute(&nb, cudaDevAttrMultiProcessorCount, h->device);
+  out[3] = nb;
+  return SNS_OK;
+}
+
 int sns_grid_size(const sns_handle* h) { return h ? h->n : 0; }
 size_t sns_device_bytes(const sns_handle* h) { return h ? h->bytes : 0; }
 
