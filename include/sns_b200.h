@@ -68,7 +68,8 @@ int sns_create(int n, double nu, int precision, int viscous_mode, uint64_t seed,
                sns_handle** out);
 int sns_destroy(sns_handle* h);
 
-/* Message of the last failed call on h (or of the last failed sns_create when h is NULL). */
+/* Message of the last failed call on h (or, when h is NULL, of the last failed call made
+ * without a handle: sns_create, sns_forward_r2c_noalloc). */
 const char* sns_last_error(const sns_handle* h);
 
 /* FFT-backend contract (FftwFft3D::forward / backward, src/fftw_fft.cpp:53-85):
@@ -125,6 +126,22 @@ int sns_time_steps(sns_handle* h, double dt, int nsteps, double* elapsed_ms);
  * k-space sweep.  Benchmark/profiling aid; not for timed runs. */
 #define SNS_NUM_PASSES 7
 int sns_profile_passes(sns_handle* h, double dt, int nsteps, double* pass_ms);
+
+/* Forward transform that allocates no device memory (no counterpart in the reference).
+ * For callers that cannot let a library call cudaMalloc: applications that reserve the
+ * GPU's memory up front and serve it from their own pool, runs close to the HBM limit,
+ * and loops that cannot take the device-wide synchronisation an allocation may cause.
+ * Same result as sns_forward_r2c, but on device buffers the caller owns:
+ *   dev_physical: N^3 doubles (x fastest), dev_spectral: 2*N^3 doubles (16-byte aligned),
+ * both on the current device; stream is a cudaStream_t (NULL = the default stream) and the
+ * call returns after the work on it finished.  N <= SNS_NOALLOC_MAX_N (sizes 8 12 16 24 32
+ * 48 64); larger grids return SNS_ERR_UNSUPPORTED.  The intermediate spectrum lives in one
+ * fixed __device__ array (about 2.5 MiB) that every GPU loading the library holds until
+ * exit and that all calls on a device share: calls whose GPU work overlaps race on it.
+ * The first call on a device sets that array up (with the device current); make it before
+ * any stream capture begins.  Errors: sns_last_error(NULL). */
+#define SNS_NOALLOC_MAX_N 64
+int sns_forward_r2c_noalloc(int n, const double* dev_physical, double* dev_spectral, void* stream);
 
 /* Test hook: the k-th following call into the handle fails with SNS_ERR_INJECTED
  * (k <= 0 disables).  Exercises the error paths without touching the GPU. */

@@ -62,6 +62,7 @@ SIGNATURES = {
     "sns_time_steps": (C.c_int, [_H, C.c_double, C.c_int, _DP]),
     "sns_debug_fail_after": (C.c_int, [_H, C.c_int]),
     "sns_profile_passes": (C.c_int, [_H, C.c_double, C.c_int, _DP]),
+    "sns_forward_r2c_noalloc": (C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
 }
 
 PASS_NAMES = ("p1_zinv_phase", "p2_yinv", "p3_xpass", "p3_nyq", "p4_yfwd", "p5_zfwd", "p5_sweep")

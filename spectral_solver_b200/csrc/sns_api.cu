@@ -41,6 +41,29 @@ thread_local std::string g_create_error;
 
 }  // namespace
 
+namespace sns {
+
+// exp(-2*pi*i*t/L) for t < L, rounded from long double; exact at the quarter points.
+void fill_twiddles(int L, double2* tw) {
+  for (int t = 0; t < L; ++t) {
+    const int q = (4 * t) % (4 * L);
+    if (q % L == 0) {
+      const int k = q / L;  // t*4/L in {0,1,2,3}
+      const double c[4] = {1.0, 0.0, -1.0, 0.0};
+      const double s[4] = {0.0, -1.0, 0.0, 1.0};
+      tw[t] = make_double2(c[k], s[k]);
+    } else {
+      const long double a = -2.0L * 3.141592653589793238462643383279502884L * (long double)t / (long double)L;
+      tw[t] = make_double2((double)cosl(a), (double)sinl(a));
+    }
+  }
+}
+
+// Message slot that sns_last_error(NULL) reads: failures of calls made without a handle.
+void set_handleless_error(const char* msg) { g_create_error = msg; }
+
+}  // namespace sns
+
 struct sns_handle {
   int n = 0;
   int device = 0;
@@ -91,21 +114,9 @@ size_t partial_slots(int n) {
   return 2 * rows + 4096;
 }
 
-// exp(-2*pi*i*t/L) rounded from long double; exact at the quarter points.
 std::vector<double2> twiddle_table(int L) {
   std::vector<double2> tw(L);
-  for (int t = 0; t < L; ++t) {
-    const int q = (4 * t) % (4 * L);
-    if (q % L == 0) {
-      const int k = q / L;  // t*4/L in {0,1,2,3}
-      const double c[4] = {1.0, 0.0, -1.0, 0.0};
-      const double s[4] = {0.0, -1.0, 0.0, 1.0};
-      tw[t] = make_double2(c[k], s[k]);
-    } else {
-      const long double a = -2.0L * 3.141592653589793238462643383279502884L * (long double)t / (long double)L;
-      tw[t] = make_double2((double)cosl(a), (double)sinl(a));
-    }
-  }
+  sns::fill_twiddles(L, tw.data());
   return tw;
 }
 

@@ -96,6 +96,10 @@ void launch_full_to_half(const double2* full, double2* half, int hermitian_part,
 void launch_spectral_diag(const double2* u, double* partials, int nblocks, Geom g, cudaStream_t st);
 void launch_reduce(const double* partials, int count, int stride, int op_max, double* out, cudaStream_t st);
 
+// Host helpers shared by the C-ABI files (sns_api.cu).
+void fill_twiddles(int L, double2* tw);        // exp(-2*pi*i*t/L), t < L
+void set_handleless_error(const char* msg);    // message for sns_last_error(NULL)
+
 constexpr int kXDiagPartials = 2;   // (sum 0.5|u|^2, max |u|^2) per row
 constexpr int kSpecDiagPartials = 2;  // (sum w*|H(omega)|^2, max |k.u|) per block
 
