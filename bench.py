@@ -2,13 +2,18 @@
 """Benchmark of the pseudo-spectral Taylor-Green RK3 step on B200.
 
 Workload (one "step" = one low-storage RK3 step over the whole grid): Taylor-Green vortex,
-N = 512^3, FP64 plain form (the reference's scheme: phase-shift dealiasing, sphere
-truncation, explicit viscosity, Williamson RK3), Re = 1600, dt = 1e-3.  The state stays
-resident in HBM (19.9 GB, far above the 126 MB L2, so no L2 flush is needed).
+N = 512^3 (the reference's scheme: phase-shift dealiasing, sphere truncation, explicit
+viscosity, Williamson RK3), Re = 1600, dt = 1e-3, in two forms measured in the same run:
+the FP32 precision ("mixed") form -- fields in FP32, twiddles / phases generated in FP64,
+energy / enstrophy / dissipation reductions in FP64 -- is the headline `value`; the FP64
+plain drop-in form runs beside it (`fp64_plain`, `mixed_vs_fp64`), and the gap between the
+two forms' E and eps after the same steps is reported (`mixed_error_vs_fp64`).  The state
+stays resident in HBM (10 GB FP32, 20 GB FP64: far above the 126 MB L2, so no L2 flush).
 
 Metric: grid-point * RK3-steps per second, in units of 1e9 (Gpt*RK3-steps/s).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--n 512]
+                    [--precision both|fp32|fp64]
 
 With --gpus N > 1 (torchrun, one rank per GPU) every rank steps its own replica (the
 path does not shard without an all-to-all transpose, so multi-GPU is replicas only);
@@ -47,6 +52,8 @@ LAUNCHES_PER_STEP = 3 * 6
 TRAFFIC_PER_POINT = {"p5_sweep": 3.262e9 / 256 ** 3, "p3_xpass": 2.445e9 / 256 ** 3,
                      "p4_yfwd": 3.268e9 / 256 ** 3, "p1_zinv_phase": 1.166e9 / 256 ** 3,
                      "p2_yinv": 1.582e9 / 256 ** 3}
+# The same for the FP32 precision form (filled from its own captures).
+TRAFFIC_PER_POINT_FP32 = {}
 
 
 def load_peaks():
@@ -195,42 +202,52 @@ def run_reference(args, world, rank, pg):
     return 0
 
 
-def run_b200(args, world, rank, local, pg):
-    import numpy as np
-    import torch
+def measure_form(args, n, precision, local, pg):
+    """Time one form (FP64 plain or FP32 precision) of the step on this rank: warm-up, K
+    timed steps on the library's stream with CUDA events, per-pass event times.  Returns
+    (solver, dict)."""
     from spectral_solver_b200 import Solver
-
-    n = args.n
-    torch.cuda.set_device(local)
-    s = Solver(n, RE)
-    # warm-up (untimed)
-    s.step(DT, args.warmup)
+    s = Solver(n, RE, precision=precision)
+    s.step(DT, args.warmup)  # warm-up (untimed)
     barrier_sync(pg)
     with ClockSampler(local) as clk:
         ms = s.time_steps(DT, args.steps)  # CUDA events on the library's launching stream
     barrier_sync(pg)
     clocks = clk.summary()
     ms_max = max_over_ranks(pg, ms)
+    world = int(os.environ.get("WORLD_SIZE", "1"))
     units = world * n ** 3 * args.steps
     value = units / (ms_max / 1e3) / 1e9
-
     # Per-pass device times (events between passes, separate from the timed region).
     prof = s.profile_passes(DT, 1)
-    S = n ** 3 * 8
+    w = 8 if precision == 0 else 4
+    S = n ** 3 * w
     top = max(prof, key=prof.get)
     achieved = PASS_BYTES_S[top] * S / (prof[top] / 1e3) / 1e9
     peak, peak_kind = load_peaks()
+    traffic_table = TRAFFIC_PER_POINT if precision == 0 else TRAFFIC_PER_POINT_FP32
+    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": (traffic_table[top] * n ** 3) if top in traffic_table else None,
+            "kernel": top, "peak_source": f"hbm_gbs {peak_kind}",
+            "algorithmic_bytes_per_launch": PASS_BYTES_S[top] * S, "mean_launch_ms": prof[top]}
+    return s, {"value": value, "ms_per_step": ms_max / args.steps, "clocks": clocks, "roofline": roof,
+               "passes_ms_per_stage": prof, "model_roofline_frac": value / (peak / (261 * w)),
+               "steps_done": args.warmup + args.steps + 1}
 
-    # End to end through the C ABI with host buffers: upload the initial spectral state from
-    # pinned host memory, K steps each followed by a diagnostics row read back to the host,
-    # then the final physical velocity read back -- a whole solve from the user's side.
+
+def e2e_solve(args, s, n, pg):
+    """End to end through the C ABI with host buffers: upload the initial spectral state from
+    pinned host memory, K steps each followed by a diagnostics row read back to the host,
+    then the final physical velocity read back -- a whole solve from the user's side."""
+    import ctypes as C
+    import numpy as np
+    import torch
+    from spectral_solver_b200 import _lib
     state = s.get_state()
     pin = [torch.empty(2 * n ** 3, dtype=torch.float64, pin_memory=True) for _ in range(3)]
     for c in range(3):
         pin[c].numpy()[:] = state[c].view(np.float64).reshape(-1)
     out = [torch.empty(n ** 3, dtype=torch.float64, pin_memory=True) for _ in range(3)]
-    import ctypes as C
-    from spectral_solver_b200 import _lib
     lib = _lib.load()
     DP = C.POINTER(C.c_double)
     ins = (DP * 3)(*[C.cast(p.data_ptr(), DP) for p in pin])
@@ -249,10 +266,31 @@ def run_b200(args, world, rank, local, pg):
     if rc != 0:
         raise RuntimeError("e2e run failed: " + lib.sns_last_error(s.h).decode())
     e2e_s = max_over_ranks(pg, e2e_s)
-    e2e_value = units / e2e_s / 1e9
-    h2d = 3 * 2 * n ** 3 * 8 / args.steps
-    d2h = (3 * n ** 3 * 8 + args.steps * 4 * 8) / args.steps
-    s.close()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    units = world * n ** 3 * args.steps
+    return {"value": units / e2e_s / 1e9, "unit": UNIT,
+            "h2d_bytes_per_step": 3 * 2 * n ** 3 * 8 / args.steps,
+            "d2h_bytes_per_step": (3 * n ** 3 * 8 + args.steps * 6 * 8) / args.steps,
+            "what": "set_state from pinned host + K x (step + diagnostics row to host) + final velocity to host"}
+
+
+def run_b200(args, world, rank, local, pg):
+    import torch
+
+    n = args.n
+    torch.cuda.set_device(local)
+    forms = {"fp64": 0, "fp32": 1} if args.precision == "both" else {args.precision: 0 if args.precision == "fp64" else 1}
+    results, diags = {}, {}
+    head = "fp32" if "fp32" in forms else "fp64"
+    e2e = None
+    for name, prec in forms.items():
+        s, r = measure_form(args, n, prec, local, pg)
+        # both forms started from the same Taylor-Green field and took the same steps
+        diags[name] = s.diagnostics(DT * r["steps_done"])
+        if name == head:
+            e2e = e2e_solve(args, s, n, pg)
+        s.close()
+        results[name] = r
 
     if rank == 0:
         cpu = None
@@ -260,31 +298,40 @@ def run_b200(args, world, rank, local, pg):
             rate, secs, threads = cpu_oracle_rate(n, 1)
             cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
                    "sample": f"1 RK3 stage at {n}^3 ({secs:.1f} s) of the CPU oracle (oracle/ref_r2c.py, scipy "
-                             f"pocketfft, {threads} threads); the reference's FFTW path cannot be built here"}
+                             f"pocketfft, {threads} threads, FP64); the reference's FFTW path cannot be built here"}
+        r = results[head]
+        cb = 16 if head == "fp64" else 8
+        resident = 18 * n * n * (((n // 2 + 1) + 128 // cb - 1) // (128 // cb) * (128 // cb)) * cb / 1e9
         line = {
-            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": r["ms_per_step"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 (FP64 twiddles, IF exponent and reductions)" if head == "fp32" else "f64",
             "data": "synthetic: analytic Taylor-Green initial field (Re=1600)",
-            "config": {"workload": f"Taylor-Green RK3 step, {n}^3, FP64 plain drop-in form "
-                                   "(phase-shift dealiasing, sphere truncation, explicit viscosity)",
-                       "n": n, "precision": "fp64", "reynolds": RE, "dt": DT,
+            "config": {"workload": f"Taylor-Green RK3 step, {n}^3, "
+                                   + ("FP32 precision form (mixed)" if head == "fp32" else "FP64 plain drop-in form")
+                                   + " (phase-shift dealiasing, sphere truncation, explicit viscosity)",
+                       "n": n, "precision": head, "reynolds": RE, "dt": DT,
                        "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
-                       "l2": f"inputs larger than L2 ({(18 * n * n * (((n // 2 + 1) + 7) // 8 * 8) * 16) / 1e9:.1f} GB resident)"},
-            "clocks": clocks,
+                       "l2": f"inputs larger than L2 ({resident:.1f} GB resident)"},
+            "clocks": r["clocks"],
             "gpu_launches": LAUNCHES_PER_STEP * args.steps,
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak,
-                         "traffic": (TRAFFIC_PER_POINT[top] * n ** 3) if top in TRAFFIC_PER_POINT else None,
-                         "kernel": top,
-                         "peak_source": f"hbm_gbs {peak_kind}",
-                         "algorithmic_bytes_per_launch": PASS_BYTES_S[top] * S,
-                         "mean_launch_ms": prof[top]},
-            "passes_ms_per_stage": prof,
-            "model_roofline_frac": value / (peak / (261 * 8)),
-            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                    "what": "set_state from pinned host + K x (step + diagnostics row to host) + final velocity to host"},
+            "roofline": r["roofline"],
+            "passes_ms_per_stage": r["passes_ms_per_stage"],
+            "model_roofline_frac": r["model_roofline_frac"],
+            "e2e": e2e,
         }
+        if "fp64" in results and head != "fp64":
+            f64 = results["fp64"]
+            line["fp64_plain"] = {k: f64[k] for k in ("value", "ms_per_step", "model_roofline_frac", "roofline",
+                                                        "passes_ms_per_stage", "clocks")}
+            line["mixed_vs_fp64"] = r["value"] / f64["value"]
+            d32, d64 = diags["fp32"], diags["fp64"]
+            line["mixed_error_vs_fp64"] = {
+                "after_steps": r["steps_done"],
+                "abs_kinetic_energy": abs(d32["kinetic_energy"] - d64["kinetic_energy"]),
+                "abs_dissipation": abs(d32["dissipation"] - d64["dissipation"]),
+                "rel_enstrophy": abs(d32["enstrophy"] - d64["enstrophy"]) / d64["enstrophy"]}
         if cpu is not None:
             line["cpu_baseline"] = cpu
         print(json.dumps(line), flush=True)
@@ -299,6 +346,8 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--n", type=int, default=512)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--precision", default="both", choices=["both", "fp32", "fp64"],
+                    help="both: the FP32 precision form is the headline, the FP64 plain form runs beside it")
     args = ap.parse_args()
     if args.impl == "reference":
         # CPU-only arm: no process group; under torchrun rank 0 alone runs

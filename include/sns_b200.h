@@ -36,8 +36,17 @@ enum {
   SNS_ERR_INJECTED = 6        /* failure forced by sns_debug_fail_after (tests only) */
 };
 
-enum { SNS_PRECISION_FP64 = 0 };
-enum { SNS_VISCOUS_EXPLICIT = 0 };
+/* Storage precision of a solver: FP64 plain form (the drop-in), or the FP32 precision form
+ * (fields in FP32; twiddles and phases generated in FP64 and rounded; energy, enstrophy,
+ * dissipation and the Nyquist-plane sums accumulated in FP64).  Host buffers are doubles
+ * for both. */
+enum { SNS_PRECISION_FP64 = 0, SNS_PRECISION_FP32 = 1 };
+/* Viscous treatment: the reference's explicit term -nu*k^2*u_hat inside the RHS (the drop-in),
+ * or an integrating factor: the RHS is the projected nonlinear term alone and each RK3
+ * stage multiplies u_hat and g by exp(-nu*k^2*(c_{s+1} - c_s)*dt), stage times
+ * c = (0, 1/3, 3/4, 1), exponent evaluated in FP64.  In that mode sns_rhs returns the
+ * projected nonlinear term (the RHS of the transformed equation at the current time). */
+enum { SNS_VISCOUS_EXPLICIT = 0, SNS_VISCOUS_INTEGRATING_FACTOR = 1 };
 
 typedef struct sns_handle sns_handle;
 
@@ -55,7 +64,8 @@ typedef struct sns_diag {
 /* Library version string. */
 const char* sns_version(void);
 
-/* Bytes of device memory a solver handle of size n needs (state + work + tables). */
+/* Bytes of device memory a solver handle of size n and the given precision needs
+ * (state + work + tables); 0 for an unknown precision. */
 size_t sns_bytes_required(int n, int precision);
 
 /* Create a solver: Taylor-Green initial field (u = sin x cos y cos z, v = -cos x sin y cos z,

@@ -1,8 +1,9 @@
 // TaylorGreenSolver / run_taylor_green over the B200 backend: the reference's benchmarked
 // AVA solver interface (src/ava_taylor_green.hpp:8-55 of ovankerm/Spectral_solver) with
 // the same records, constructor, methods, run options, CSV columns and stdout lines.
-// RunConfig gains optional fields for the seeded perturbation and the final-field dump;
-// their defaults reproduce the reference's run.
+// RunConfig gains optional fields for the seeded perturbation, the final-field dump, the
+// storage precision and the viscous treatment; their defaults reproduce the reference's run
+// (the reference picks its precision at build time through SPECTRAL_PRECISION).
 #pragma once
 
 #include <cstdint>
@@ -44,6 +45,8 @@ struct RunConfig {
   double pert_amp = 0.0;
   int pert_kmax = 0;
   bool dump_final = false;
+  int precision = 0;     // 0: FP64 plain form (the drop-in), 1: FP32 precision form
+  int viscous_mode = 0;  // 0: explicit viscous term (the reference), 1: integrating factor
 };
 
 class TaylorGreenSolver {
@@ -51,7 +54,8 @@ class TaylorGreenSolver {
   struct Impl;
 
   TaylorGreenSolver(int n, double reynolds);
-  TaylorGreenSolver(int n, double reynolds, std::uint64_t seed, double pert_amp, int pert_kmax);
+  TaylorGreenSolver(int n, double reynolds, std::uint64_t seed, double pert_amp, int pert_kmax, int precision = 0,
+                    int viscous_mode = 0);
   ~TaylorGreenSolver();
 
   TaylorGreenSolver(const TaylorGreenSolver&) = delete;

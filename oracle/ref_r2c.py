@@ -61,13 +61,15 @@ def half_to_full(h: np.ndarray) -> np.ndarray:
 class TaylorGreenR2C:
     """Half-spectrum restatement of ``TaylorGreenSolver::Impl`` with identical numerics."""
 
-    def __init__(self, n: int, reynolds: float, u_hat0=None, workers: int | None = None):
+    def __init__(self, n: int, reynolds: float, u_hat0=None, workers: int | None = None,
+                 integrating_factor: bool = False):
         if n <= 0:
             raise ValueError("grid size must be positive")
         if reynolds <= 0.0:
             raise ValueError("Reynolds number must be positive")
         self.n = n
         self.nu = 1.0 / reynolds
+        self.integrating_factor = integrating_factor
         self.global_size = n * n * n
         self.workers = WORKERS if workers is None else workers
         mx, my, mz = half_mode_grids(n)
@@ -135,10 +137,20 @@ class TaylorGreenR2C:
         if u_hat is None:
             u_hat = self.u_hat
         rhs = self.nonlinear(u_hat)
-        for c in range(3):
-            rhs[c] = rhs[c] - u_hat[c] * (self.nu * self.k2)
+        if not self.integrating_factor:
+            for c in range(3):
+                rhs[c] = rhs[c] - u_hat[c] * (self.nu * self.k2)
         self.project_truncate(rhs)
         return rhs
+
+    def _if_advance(self, u, g, tau):
+        # Integrating-factor variant (an option the reference's method notes list, doc.md:325-343,
+        # but do not implement): u and g are carried to the next stage time by exp(-nu k^2 tau).
+        if self.integrating_factor:
+            f = np.exp(-self.nu * self.k2 * tau)
+            for c in range(3):
+                u[c] = u[c] * f
+                g[c] = g[c] * f
 
     def step(self, dt: float):
         u, g = self.u_hat, self.g
@@ -146,16 +158,19 @@ class TaylorGreenR2C:
         for c in range(3):
             g[c] = r[c].copy()
             u[c] = u[c] + g[c] * (dt / 3.0)
+        self._if_advance(u, g, dt / 3.0)
         self.project_truncate(u)
         r = self.compute_rhs()
         for c in range(3):
             g[c] = g[c] * (-5.0 / 9.0) + r[c]
             u[c] = u[c] + g[c] * (15.0 * dt / 16.0)
+        self._if_advance(u, g, 5.0 * dt / 12.0)
         self.project_truncate(u)
         r = self.compute_rhs()
         for c in range(3):
             g[c] = g[c] * (-153.0 / 128.0) + r[c]
             u[c] = u[c] + g[c] * (8.0 * dt / 15.0)
+        self._if_advance(u, g, dt / 4.0)
         self.project_truncate(u)
 
     step_rk3 = step

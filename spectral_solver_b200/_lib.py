@@ -21,6 +21,7 @@ SNS_ERR_NOMEM = 4
 SNS_ERR_NO_DEVICE = 5
 SNS_ERR_INJECTED = 6
 PRECISION_FP64 = 0
+PRECISION_FP32 = 1
 VISCOUS_EXPLICIT = 0
 
 # Every symbol include/sns_b200.h declares, with its ctypes signature.
@@ -114,13 +115,14 @@ class Solver:
     """Thin RAII wrapper of an ``sns_handle`` (Python mirror of TaylorGreenSolver)."""
 
     def __init__(self, n: int, reynolds: float = 1600.0, seed: int = 0, pert_amp: float = 0.0,
-                 pert_kmax: int = 0, nu: float | None = None):
+                 pert_kmax: int = 0, nu: float | None = None, precision: int = PRECISION_FP64,
+                 viscous_mode: int = VISCOUS_EXPLICIT):
         self.lib = load()
         self.n = n
+        self.precision = precision
         self.nu = (1.0 / reynolds) if nu is None else nu
         h = _H()
-        rc = self.lib.sns_create(n, self.nu, PRECISION_FP64, VISCOUS_EXPLICIT, seed, pert_amp, pert_kmax,
-                                 C.byref(h))
+        rc = self.lib.sns_create(n, self.nu, precision, viscous_mode, seed, pert_amp, pert_kmax, C.byref(h))
         if rc != SNS_OK:
             raise SnsError(rc, self.lib.sns_last_error(None).decode())
         self.h = h

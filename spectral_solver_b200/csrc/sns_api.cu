@@ -1,6 +1,7 @@
 // C ABI of the B200 Taylor-Green solver: handle, device memory, tables, step orchestration.
 //
-// Device memory of a handle (FP64 plain form), in half fields of N*N*pitch double2:
+// Device memory of a handle, in half fields of N*N*pitch complex values (double2 in the FP64
+// plain form, float2 in the FP32 precision form):
 //   state : u[3], g[3]            (the reference's u_hat and g, ava_taylor_green_impl.hpp:665-667)
 //   work  : 12 fields             (inverse-transformed velocity on both grids, then the
 //                                  12 product spectra; the fused x pass reads 6 and writes
@@ -74,17 +75,19 @@ struct sns_handle {
   const sns::Ops* ops = nullptr;
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-  double2* state = nullptr;  // u[3] then g[3]
-  double2* work = nullptr;   // 12 fields
-  double2* tw = nullptr;
-  double2* phase = nullptr;
+  int cbytes = 16;          // bytes per complex value: 16 (FP64) or 8 (FP32)
+  size_t fbytes = 0;        // bytes per half field
+  char* state = nullptr;    // u[3] then g[3]
+  char* work = nullptr;     // 12 fields
+  void* tw = nullptr;
+  void* phase = nullptr;
   double* partials = nullptr;
   double* red = nullptr;  // reduction results
   int* err_word = nullptr;  // device error word written by bounded waits
   int tma_grid = 0;         // persistent CTAs of the TMA passes
   int x2_grid = 0;          // persistent CTAs of the two-stage x pass (0: generic x pass)
   int p5_grid = 0;          // persistent CTAs of the fused forward-z + sweep pass (0: two kernels)
-  double2* tw2 = nullptr;   // W_N^(r*j), r < N/16, j < 16 (two-stage x pass)
+  void* tw2 = nullptr;      // W_N^(r*j), r < N/16, j < 16 (two-stage x pass)
   double* nyq_part = nullptr;  // [12][max(1, x2_grid)] Nyquist-plane partial sums
   CUtensorMap map_state_z{};  // state fields (u[3], g[3]), z-pencil boxes
   CUtensorMap map_work_y{};   // 12 work fields, y-pencil boxes
@@ -97,17 +100,36 @@ struct sns_handle {
   bool nyq_clean = true;
   std::string err;
 
-  double2* u() const { return state; }
-  double2* gb() const { return state + 3 * g.field; }
-  double2* wf(int i) const { return work + (long long)i * g.field; }
-  int tiles_data() const { return (g.nh + 7) / 8; }   // columns [0, N/2)
-  int tiles_all() const { return g.pitch / 8; }        // Nyquist column included
+  char* u() const { return state; }
+  char* gb() const { return state + 3 * fbytes; }
+  char* ucomp(int c) const { return state + (size_t)c * fbytes; }
+  char* wf(int i) const { return work + (size_t)i * fbytes; }
+  int tcols() const { return ops->tile_cols; }
+  int tiles_data() const { return (g.nh + tcols() - 1) / tcols(); }  // columns [0, N/2)
+  int tiles_all() const { return g.pitch / tcols(); }                // Nyquist column included
   double inv_size() const { return 1.0 / ((double)n * n * n); }
 };
 
 namespace {
 
-size_t field_bytes(int n) { return (size_t)n * n * sns::pitch_for(n) * sizeof(double2); }
+int complex_bytes(int precision) { return precision == SNS_PRECISION_FP32 ? 8 : 16; }
+size_t field_bytes(int n, int precision) {
+  const int cb = complex_bytes(precision);
+  return (size_t)n * n * sns::pitch_for(n, cb) * cb;
+}
+
+// Device copy of a complex table given in FP64: as is, or rounded to FP32.
+void upload_table(void* dst, const std::vector<double2>& t, int precision, cudaStream_t st) {
+  if (precision == SNS_PRECISION_FP32) {
+    std::vector<float2> f(t.size());
+    for (size_t i = 0; i < t.size(); ++i) f[i] = make_float2((float)t[i].x, (float)t[i].y);
+    ck(cudaMemcpyAsync(dst, f.data(), f.size() * sizeof(float2), cudaMemcpyHostToDevice, st), "table upload");
+    ck(cudaStreamSynchronize(st), "table upload");
+  } else {
+    ck(cudaMemcpyAsync(dst, t.data(), t.size() * sizeof(double2), cudaMemcpyHostToDevice, st), "table upload");
+    ck(cudaStreamSynchronize(st), "table upload");
+  }
+}
 
 size_t partial_slots(int n) {
   const size_t rows = (size_t)n * n;
@@ -215,24 +237,26 @@ EncodeTiled encode_fn() {
   return fn;
 }
 
-// Tensor map over `nf` consecutive half fields viewed as [field][z][y][2*pitch doubles],
-// box = 16 doubles (8 complex, 128 bytes) x up to 256 rows along y (axis 1) or z (axis 2).
-CUtensorMap make_field_map(void* base, int nf, int axis, const sns::Geom& g) {
+// Tensor map over `nf` consecutive half fields viewed as [field][z][y][2*pitch reals],
+// box = 128 bytes (16 doubles = 8 complex, or 32 floats = 16 complex) x up to 256 rows
+// along y (axis 1) or z (axis 2).
+CUtensorMap make_field_map(void* base, int nf, int axis, const sns::Geom& g, int cbytes) {
   CUtensorMap m;
-  const cuuint64_t row = (cuuint64_t)g.pitch * sizeof(double2);
+  const cuuint64_t row = (cuuint64_t)g.pitch * cbytes;
   cuuint64_t dims[4] = {(cuuint64_t)2 * g.pitch, (cuuint64_t)g.n, (cuuint64_t)g.n, (cuuint64_t)nf};
-  cuuint64_t strides[3] = {row, row * g.n, (cuuint64_t)g.field * sizeof(double2)};
+  cuuint64_t strides[3] = {row, row * g.n, (cuuint64_t)g.field * cbytes};
   const cuuint32_t br = g.n < 256 ? (cuuint32_t)g.n : 256u;
-  cuuint32_t box[4] = {16u, axis == 1 ? br : 1u, axis == 2 ? br : 1u, 1u};
+  cuuint32_t box[4] = {(cuuint32_t)(256 / cbytes), axis == 1 ? br : 1u, axis == 2 ? br : 1u, 1u};
   cuuint32_t es[4] = {1u, 1u, 1u, 1u};
-  const CUresult r = encode_fn()(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, base, dims, strides, box, es,
+  const CUtensorMapDataType dt = cbytes == 16 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+  const CUresult r = encode_fn()(&m, dt, 4, base, dims, strides, box, es,
                                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                                  CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) throw SnsError(SNS_ERR_CUDA, "cuTensorMapEncodeTiled failed: " + std::to_string((int)r));
   return m;
 }
 
-sns::TmaArgs tma_args(sns_handle* h, int f_in0, int nf, int ncb, double2* out, int f_out0, double scale) {
+sns::TmaArgs tma_args(sns_handle* h, int f_in0, int nf, int ncb, void* out, int f_out0, double scale) {
   sns::TmaArgs a;
   a.f_in0 = f_in0;
   a.nf = nf;
@@ -273,13 +297,13 @@ inline void mark(PassMarks* pm, int i, cudaStream_t st) {
 }
 
 // One RK3 stage (or the RHS only, mode 1) on u_src: the five fused passes.
-void run_stage(sns_handle* h, double2* u_src, double2* g_buf, int stage, double dt, int mode, double2* rhs_out,
+void run_stage(sns_handle* h, char* u_src, char* g_buf, int stage, double dt, int mode, char* rhs_out,
                double* partials, PassMarks* pm = nullptr) {
   const sns::Ops* o = h->ops;
   const sns::Geom& g = h->g;
   cudaStream_t st = h->stream;
   const int tiles_in = h->nyq_clean ? h->tiles_data() : h->tiles_all();
-  const int f_src = (int)((u_src - h->state) / g.field);  // u (0) or the g slot (3)
+  const int f_src = (int)((size_t)(u_src - h->state) / h->fbytes);  // u (0) or the g slot (3)
   mark(pm, 0, st);
   o->yz_tma(h->map_state_z, 2, +1, 1, tma_args(h, f_src, 3, tiles_in, h->work, 0, h->inv_size()), h->tw, h->phase,
             g, h->tma_grid, st);
@@ -312,6 +336,10 @@ void run_stage(sns_handle* h, double2* u_src, double2* g_buf, int stage, double 
   a.stage = stage;
   a.mode = mode;
   a.dealias = 1;
+  // integrating-factor mode: after stage s, u and g advance from c_s*dt to c_{s+1}*dt with
+  // the stage times c = (0, 1/3, 3/4, 1) of the Williamson scheme
+  a.visc_if = h->viscous_mode == SNS_VISCOUS_INTEGRATING_FACTOR ? 1 : 0;
+  a.if_tau = stage == 0 ? dt / 3.0 : (stage == 1 ? 5.0 * dt / 12.0 : dt / 4.0);
   if (stage == 0) {
     a.ga = 0.0;
     a.ub = dt / 3.0;
@@ -350,17 +378,18 @@ bool nyquist_plane_dirty(int n, const double* full) {
 }
 
 // Upload a reference full-layout field into half field `dst` (optionally Hermitian part).
-void upload_full(sns_handle* h, const double* host, double2* dst, int herm) {
-  double2* staging = h->wf(4);  // N^3 double2 fit in work fields 4..(4 + N/pitch)
+// The N^3 complex doubles of a full-layout field fit in work fields 4..11 for either precision.
+void upload_full(sns_handle* h, const double* host, void* dst, int herm) {
+  double2* staging = reinterpret_cast<double2*>(h->wf(4));
   const size_t bytes = (size_t)h->n * h->n * h->n * sizeof(double2);
   ck(cudaMemcpyAsync(staging, host, bytes, cudaMemcpyHostToDevice, h->stream), "upload");
-  sns::launch_full_to_half(staging, dst, herm, h->g, h->stream);
+  sns::launch_full_to_half(staging, dst, h->precision, herm, h->g, h->stream);
 }
 
-void download_full(sns_handle* h, const double2* src, double* host) {
-  double2* staging = h->wf(4);
+void download_full(sns_handle* h, const void* src, double* host) {
+  double2* staging = reinterpret_cast<double2*>(h->wf(4));
   const size_t bytes = (size_t)h->n * h->n * h->n * sizeof(double2);
-  sns::launch_half_to_full(src, staging, h->g, h->stream);
+  sns::launch_half_to_full(src, h->precision, staging, h->g, h->stream);
   ck(cudaMemcpyAsync(host, staging, bytes, cudaMemcpyDeviceToHost, h->stream), "download");
 }
 
@@ -424,11 +453,12 @@ void release(sns_handle* h) {
 
 extern "C" {
 
-const char* sns_version(void) { return "sns_b200 0.1 (sm_100a, fp64 plain form)"; }
+const char* sns_version(void) { return "sns_b200 0.2 (sm_100a, fp64 plain form, fp32 precision form)"; }
 
 size_t sns_bytes_required(int n, int precision) {
-  if (n <= 0 || precision != SNS_PRECISION_FP64) return 0;
-  return 18 * field_bytes(n) + partial_slots(n) * sizeof(double) + (size_t)(4 * n + 64) * sizeof(double2);
+  if (n <= 0 || (precision != SNS_PRECISION_FP64 && precision != SNS_PRECISION_FP32)) return 0;
+  return 18 * field_bytes(n, precision) + partial_slots(n) * sizeof(double) +
+         (size_t)(4 * n + 64) * complex_bytes(precision);
 }
 
 int sns_create(int n, double nu, int precision, int viscous_mode, uint64_t seed, double pert_amp, int pert_kmax,
@@ -447,15 +477,15 @@ int sns_create(int n, double nu, int precision, int viscous_mode, uint64_t seed,
     g_create_error = "viscosity must be finite and non-negative (Reynolds number must be positive)";
     return SNS_ERR_INVALID;
   }
-  if (precision != SNS_PRECISION_FP64) {
-    g_create_error = "only the FP64 plain form is built";
+  if (precision != SNS_PRECISION_FP64 && precision != SNS_PRECISION_FP32) {
+    g_create_error = "precision must be SNS_PRECISION_FP64 (0) or SNS_PRECISION_FP32 (1)";
     return SNS_ERR_UNSUPPORTED;
   }
-  if (viscous_mode != SNS_VISCOUS_EXPLICIT) {
-    g_create_error = "only the explicit viscous term (the reference's scheme) is built";
+  if (viscous_mode != SNS_VISCOUS_EXPLICIT && viscous_mode != SNS_VISCOUS_INTEGRATING_FACTOR) {
+    g_create_error = "viscous mode must be SNS_VISCOUS_EXPLICIT (0) or SNS_VISCOUS_INTEGRATING_FACTOR (1)";
     return SNS_ERR_UNSUPPORTED;
   }
-  const sns::Ops* ops = sns::ops_for(n);
+  const sns::Ops* ops = sns::ops_for(n, precision);
   if (ops == nullptr) {
     g_create_error = "grid size " + std::to_string(n) + " has no FFT plan (supported: 8 12 16 24 32 48 64 96 128 256 512)";
     return SNS_ERR_UNSUPPORTED;
@@ -482,7 +512,10 @@ int sns_create(int n, double nu, int precision, int viscous_mode, uint64_t seed,
     h->precision = precision;
     h->viscous_mode = viscous_mode;
     h->ops = ops;
-    h->g = sns::Geom{n, n / 2, sns::pitch_for(n), (long long)n * n * sns::pitch_for(n)};
+    h->cbytes = complex_bytes(precision);
+    const int pitch = sns::pitch_for(n, h->cbytes);
+    h->g = sns::Geom{n, n / 2, pitch, (long long)n * n * pitch};
+    h->fbytes = field_bytes(n, precision);
     const size_t need = sns_bytes_required(n, precision);
     size_t free_b = 0, total_b = 0;
     ck(cudaMemGetInfo(&free_b, &total_b), "cudaMemGetInfo");
@@ -492,7 +525,7 @@ int sns_create(int n, double nu, int precision, int viscous_mode, uint64_t seed,
     ck(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "cudaStreamCreate");
     ck(cudaEventCreate(&h->ev0), "cudaEventCreate");
     ck(cudaEventCreate(&h->ev1), "cudaEventCreate");
-    const size_t fb = field_bytes(n);
+    const size_t fb = h->fbytes;
     h->partial_count = partial_slots(n);
     auto alloc = [&](void** p, size_t bytes) {
       cudaError_t e = cudaMalloc(p, bytes);
@@ -504,8 +537,8 @@ int sns_create(int n, double nu, int precision, int viscous_mode, uint64_t seed,
     };
     alloc((void**)&h->state, 6 * fb);
     alloc((void**)&h->work, 12 * fb);
-    alloc((void**)&h->tw, (size_t)n * sizeof(double2));
-    alloc((void**)&h->phase, (size_t)(3 * n + 1) * sizeof(double2));
+    alloc((void**)&h->tw, (size_t)n * h->cbytes);
+    alloc((void**)&h->phase, (size_t)(3 * n + 1) * h->cbytes);
     alloc((void**)&h->partials, h->partial_count * sizeof(double));
     alloc((void**)&h->red, 16 * sizeof(double));
     alloc((void**)&h->err_word, sizeof(int));
@@ -516,24 +549,24 @@ int sns_create(int n, double nu, int precision, int viscous_mode, uint64_t seed,
     h->x2_grid = ops->xpass2_grid(nsm);
     h->p5_grid = ops->p5_grid(nsm);
     alloc((void**)&h->nyq_part, (size_t)12 * (h->x2_grid > 0 ? h->x2_grid : 1) * sizeof(double));
-    alloc((void**)&h->tw2, (size_t)n * sizeof(double2));
+    alloc((void**)&h->tw2, (size_t)n * h->cbytes);
     {
       // tw2[r*16 + j] = exp(-2*pi*i*r*j/n) for r < n/16, j < 16
       const auto tw = twiddle_table(n);
       std::vector<double2> t2((size_t)n);
       for (int r = 0; r < n / 16; ++r)
         for (int j = 0; j < 16; ++j) t2[(size_t)r * 16 + j] = tw[(size_t)(r * j) % n];
-      ck(cudaMemcpy(h->tw2, t2.data(), t2.size() * sizeof(double2), cudaMemcpyHostToDevice), "tw2");
+      upload_table(h->tw2, t2, precision, h->stream);
     }
-    h->map_state_z = make_field_map(h->state, 6, 2, h->g);
-    h->map_work_y = make_field_map(h->work, 12, 1, h->g);
-    h->map_work_z = make_field_map(h->work, 12, 2, h->g);
+    h->map_state_z = make_field_map(h->state, 6, 2, h->g, h->cbytes);
+    h->map_work_y = make_field_map(h->work, 12, 1, h->g, h->cbytes);
+    h->map_work_z = make_field_map(h->work, 12, 2, h->g, h->cbytes);
     ck(cudaMemsetAsync(h->state, 0, 6 * fb, h->stream), "memset");
     ck(cudaMemsetAsync(h->work, 0, 12 * fb, h->stream), "memset");
     const auto tw = twiddle_table(n);
     const auto ph = phase_table(n);
-    ck(cudaMemcpyAsync(h->tw, tw.data(), tw.size() * sizeof(double2), cudaMemcpyHostToDevice, h->stream), "tw");
-    ck(cudaMemcpyAsync(h->phase, ph.data(), ph.size() * sizeof(double2), cudaMemcpyHostToDevice, h->stream), "ph");
+    upload_table(h->tw, tw, precision, h->stream);
+    upload_table(h->phase, ph, precision, h->stream);
     // Initial field: TGV at cell centres -> forward transform -> + perturbation -> project_truncate.
     double* phys = reinterpret_cast<double*>(h->wf(6));
     sns::launch_tgv_init(phys, h->g, h->stream);
@@ -545,13 +578,13 @@ int sns_create(int n, double nu, int precision, int viscous_mode, uint64_t seed,
     perturbation_entries(n, seed, pert_amp, pert_kmax, h->g, idx, val);
     if (!idx.empty()) {
       long long* d_idx = reinterpret_cast<long long*>(h->wf(8));
-      double2* d_val = h->wf(9);
+      double2* d_val = reinterpret_cast<double2*>(h->wf(9));
       ck(cudaMemcpyAsync(d_idx, idx.data(), idx.size() * sizeof(long long), cudaMemcpyHostToDevice, h->stream), "p");
       ck(cudaMemcpyAsync(d_val, val.data(), val.size() * sizeof(double2), cudaMemcpyHostToDevice, h->stream), "p");
-      sns::launch_add_sparse(h->u(), d_idx, d_val, (int)idx.size(), h->stream);
+      sns::launch_add_sparse(h->u(), precision, d_idx, d_val, (int)idx.size(), h->stream);
       ck(cudaStreamSynchronize(h->stream), "perturbation");
     }
-    sns::launch_project_truncate(h->u(), h->g, h->stream);
+    sns::launch_project_truncate(h->u(), precision, h->g, h->stream);
     ck(cudaMemsetAsync(h->work, 0, 12 * fb, h->stream), "memset");
     sync(h, "sns_create");
   } catch (const SnsError& e) {
@@ -639,10 +672,10 @@ int sns_backward_c2r(sns_handle* h, const double* host_spectral, double* host_ph
 int sns_set_state(sns_handle* h, const double* const uhat_full[3]) {
   return guarded(h, [&] {
     if (!uhat_full || !uhat_full[0] || !uhat_full[1] || !uhat_full[2]) throw SnsError(SNS_ERR_INVALID, "null buffer");
-    ck(cudaMemsetAsync(h->u(), 0, 3 * field_bytes(h->n), h->stream), "memset");
+    ck(cudaMemsetAsync(h->u(), 0, 3 * h->fbytes, h->stream), "memset");
     bool dirty = false;
     for (int c = 0; c < 3; ++c) {
-      upload_full(h, uhat_full[c], h->u() + (long long)c * h->g.field, 0);
+      upload_full(h, uhat_full[c], h->ucomp(c), 0);
       dirty = dirty || nyquist_plane_dirty(h->n, uhat_full[c]);
       sync(h, "sns_set_state");
     }
@@ -654,7 +687,7 @@ int sns_get_state(sns_handle* h, double* const uhat_full[3]) {
   return guarded(h, [&] {
     if (!uhat_full || !uhat_full[0] || !uhat_full[1] || !uhat_full[2]) throw SnsError(SNS_ERR_INVALID, "null buffer");
     for (int c = 0; c < 3; ++c) {
-      download_full(h, h->u() + (long long)c * h->g.field, uhat_full[c]);
+      download_full(h, h->ucomp(c), uhat_full[c]);
       sync(h, "sns_get_state");
     }
   });
@@ -666,11 +699,11 @@ int sns_rhs(sns_handle* h, const double* const uhat_full[3], double* const rhs_f
     for (int c = 0; c < 3; ++c)
       if (!uhat_full[c] || !rhs_full[c]) throw SnsError(SNS_ERR_INVALID, "null buffer");
     // the RK scratch g doubles as the input state (g carries nothing between steps)
-    double2* uin = h->gb();
-    ck(cudaMemsetAsync(uin, 0, 3 * field_bytes(h->n), h->stream), "memset");
+    char* uin = h->gb();
+    ck(cudaMemsetAsync(uin, 0, 3 * h->fbytes, h->stream), "memset");
     bool dirty = false;
     for (int c = 0; c < 3; ++c) {
-      upload_full(h, uhat_full[c], uin + (long long)c * h->g.field, 0);
+      upload_full(h, uhat_full[c], uin + (size_t)c * h->fbytes, 0);
       dirty = dirty || nyquist_plane_dirty(h->n, uhat_full[c]);
       sync(h, "sns_rhs upload");
     }
@@ -690,11 +723,11 @@ int sns_nonlinear(sns_handle* h, const double* const uhat_full[3], double* const
     if (!uhat_full || !out_full) throw SnsError(SNS_ERR_INVALID, "null buffer");
     for (int c = 0; c < 3; ++c)
       if (!uhat_full[c] || !out_full[c]) throw SnsError(SNS_ERR_INVALID, "null buffer");
-    double2* uin = h->gb();
-    ck(cudaMemsetAsync(uin, 0, 3 * field_bytes(h->n), h->stream), "memset");
+    char* uin = h->gb();
+    ck(cudaMemsetAsync(uin, 0, 3 * h->fbytes, h->stream), "memset");
     bool dirty = false;
     for (int c = 0; c < 3; ++c) {
-      upload_full(h, uhat_full[c], uin + (long long)c * h->g.field, 0);
+      upload_full(h, uhat_full[c], uin + (size_t)c * h->fbytes, 0);
       dirty = dirty || nyquist_plane_dirty(h->n, uhat_full[c]);
       sync(h, "sns_nonlinear upload");
     }
@@ -769,7 +802,7 @@ int sns_diagnostics(sns_handle* h, double t, sns_diag* out) {
     if (!out) throw SnsError(SNS_ERR_INVALID, "null output");
     velocity_reductions(h);
     const int nb = 1184;  // 8 CTAs per SM on 148 SMs
-    sns::launch_spectral_diag(h->u(), h->partials + 2 * (size_t)h->n * h->n, nb, h->g, h->stream);
+    sns::launch_spectral_diag(h->u(), h->precision, h->partials + 2 * (size_t)h->n * h->n, nb, h->g, h->stream);
     sns::launch_reduce(h->partials + 2 * (size_t)h->n * h->n, nb, 2, 0, h->red + 2, h->stream);
     sns::launch_reduce(h->partials + 2 * (size_t)h->n * h->n + 1, nb, 2, 1, h->red + 3, h->stream);
     double r[4];

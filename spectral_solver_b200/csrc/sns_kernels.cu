@@ -1,4 +1,6 @@
-// Pass kernels of the B200 pseudo-spectral Taylor-Green step (FP64 plain form).
+// Pass kernels of the B200 pseudo-spectral Taylor-Green step.  Every kernel is generic
+// over the complex type C: double2 for the FP64 plain form, float2 for the FP32 precision
+// form (fields stored in FP32; reductions, Nyquist sums and diagnostics accumulate in FP64).
 //
 // One RK3 stage of the reference (ava_taylor_green_impl.hpp:847-977 compute_rhs plus the
 // stage update :994-1039) is five streaming passes over HBM:
@@ -23,12 +25,14 @@
 
 namespace sns {
 
-constexpr int kT = 8;  // columns per y/z tile: 8 x 16 B = one 128-byte row segment
+// Columns per y/z tile: one 128-byte row segment (8 complex doubles, 16 complex floats).
+template <class C>
+constexpr int tile_cols() { return (int)(128 / sizeof(C)); }
 
 __device__ __forceinline__ int signed_mode(int i, int n) { return i <= n / 2 ? i : i - n; }
 
-template <int N>
-__device__ __forceinline__ void load_twiddles(double2* sm_tw, const double2* tw, int tid, int nt) {
+template <int N, class C>
+__device__ __forceinline__ void load_twiddles(C* sm_tw, const C* tw, int tid, int nt) {
   for (int t = tid; t < N; t += nt) sm_tw[t] = tw[t];
 }
 
@@ -39,23 +43,25 @@ constexpr int nt_x() { return N / 2 < 32 ? 32 : (N / 2 > 256 ? 256 : N / 2); }
 
 // ------------------------------------------------------------------------------------
 // P1: inverse z transform with the fused phase shift.
-// grid (ntiles, N [my], 3 [component]); tile = 8 columns x N rows (mz).
-template <int N>
+// grid (ntiles, N [my], 3 [component]); tile = kT columns (one 128-byte row segment) x N rows (mz).
+template <int N, class C>
 __global__ void __launch_bounds__(nt_yz<N>())
-k_zpass_inv_phase(const double2* __restrict__ u, double2* __restrict__ work, const double2* __restrict__ tw,
-                  const double2* __restrict__ phase, double scale, Geom g) {
+k_zpass_inv_phase(const C* __restrict__ u, C* __restrict__ work, const C* __restrict__ tw,
+                  const C* __restrict__ phase, double scale, Geom g) {
   constexpr int NT = nt_yz<N>();
-  extern __shared__ double2 smem[];
-  double2* s_tw = smem;
-  double2* tile = smem + N;
+  constexpr int kT = tile_cols<C>();
+  extern __shared__ __align__(16) unsigned char smraw_yz[];
+  C* smem = reinterpret_cast<C*>(smraw_yz);
+  C* s_tw = smem;
+  C* tile = smem + N;
   const int tid = threadIdx.x;
   load_twiddles<N>(s_tw, tw, tid, NT);
   const int mx0 = blockIdx.x * kT;
   const int my = blockIdx.y;
   const int c = blockIdx.z;
-  const double2* src = u + (long long)c * g.field;
-  double2* dst0 = work + (long long)(2 * c) * g.field;
-  double2* dst1 = work + (long long)(2 * c + 1) * g.field;
+  const C* src = u + (long long)c * g.field;
+  C* dst0 = work + (long long)(2 * c) * g.field;
+  C* dst1 = work + (long long)(2 * c + 1) * g.field;
   for (int e = tid; e < kT * N; e += NT) {
     const int row = e / kT, col = e % kT;
     tile[e] = cscale(src[((long long)row * N + my) * g.pitch + mx0 + col], scale);
@@ -81,10 +87,10 @@ k_zpass_inv_phase(const double2* __restrict__ u, double2* __restrict__ work, con
     const bool anti = mx > 0 && mx < N / 2 && ((my == N / 2) != (row == N / 2));
     if (mx <= N / 2 && !anti) {
       const int msum = mx + smy + signed_mode(row, N);
-      const double2 v = cscale(src[((long long)row * N + my) * g.pitch + mx], scale);
+      const C v = cscale(src[((long long)row * N + my) * g.pitch + mx], scale);
       tile[e] = cmul(v, phase[msum + 3 * N / 2]);
     } else {
-      tile[e] = make_double2(0.0, 0.0);
+      tile[e] = czero<C>();
     }
   }
   __syncthreads();
@@ -96,18 +102,20 @@ k_zpass_inv_phase(const double2* __restrict__ u, double2* __restrict__ work, con
 }
 
 // y pass, in place.  grid (ntiles, N [z], nf).
-template <int N, int DIR>
+template <int N, int DIR, class C>
 __global__ void __launch_bounds__(nt_yz<N>())
-k_ypass(double2* __restrict__ f, const double2* __restrict__ tw, Geom g) {
+k_ypass(C* __restrict__ f, const C* __restrict__ tw, Geom g) {
   constexpr int NT = nt_yz<N>();
-  extern __shared__ double2 smem[];
-  double2* s_tw = smem;
-  double2* tile = smem + N;
+  constexpr int kT = tile_cols<C>();
+  extern __shared__ __align__(16) unsigned char smraw_yz[];
+  C* smem = reinterpret_cast<C*>(smraw_yz);
+  C* s_tw = smem;
+  C* tile = smem + N;
   const int tid = threadIdx.x;
   load_twiddles<N>(s_tw, tw, tid, NT);
   const int mx0 = blockIdx.x * kT;
   const int z = blockIdx.y;
-  double2* fld = f + (long long)blockIdx.z * g.field;
+  C* fld = f + (long long)blockIdx.z * g.field;
   for (int e = tid; e < kT * N; e += NT) {
     const int row = e / kT, col = e % kT;
     tile[e] = fld[((long long)z * N + row) * g.pitch + mx0 + col];
@@ -121,19 +129,21 @@ k_ypass(double2* __restrict__ f, const double2* __restrict__ tw, Geom g) {
 }
 
 // z pass, src -> dst (may alias), optional scale on load.  grid (ntiles, N [y], nf).
-template <int N, int DIR>
+template <int N, int DIR, class C>
 __global__ void __launch_bounds__(nt_yz<N>())
-k_zpass(const double2* src, double2* dst, double scale, const double2* __restrict__ tw, Geom g) {
+k_zpass(const C* src, C* dst, double scale, const C* __restrict__ tw, Geom g) {
   constexpr int NT = nt_yz<N>();
-  extern __shared__ double2 smem[];
-  double2* s_tw = smem;
-  double2* tile = smem + N;
+  constexpr int kT = tile_cols<C>();
+  extern __shared__ __align__(16) unsigned char smraw_yz[];
+  C* smem = reinterpret_cast<C*>(smraw_yz);
+  C* s_tw = smem;
+  C* tile = smem + N;
   const int tid = threadIdx.x;
   load_twiddles<N>(s_tw, tw, tid, NT);
   const int mx0 = blockIdx.x * kT;
   const int y = blockIdx.y;
-  const double2* fin = src + (long long)blockIdx.z * g.field;
-  double2* fout = dst + (long long)blockIdx.z * g.field;
+  const C* fin = src + (long long)blockIdx.z * g.field;
+  C* fout = dst + (long long)blockIdx.z * g.field;
   for (int e = tid; e < kT * N; e += NT) {
     const int row = e / kT, col = e % kT;
     tile[e] = cscale(fin[((long long)row * N + y) * g.pitch + mx0 + col], scale);
@@ -149,8 +159,8 @@ k_zpass(const double2* src, double2* dst, double scale, const double2* __restric
 
 // ------------------------------------------------------------------------------------
 // Streaming y/z pass, persistent and TMA-fed.  Each CTA walks tiles (field, fixed
-// coordinate, 8-column block) with stride gridDim.x.  A tile (8 columns x N rows,
-// 128 bytes per row) lands in one of two shared-memory input buffers through
+// coordinate, TW-column block) with stride gridDim.x.  A tile (TW = 8 complex doubles or
+// 16 complex floats x N rows, 128 bytes per row) lands in one of two shared-memory input buffers through
 // cp.async.bulk.tensor (no multicast) while the previous tile is transformed, so HBM
 // reads overlap the FFT.  The first radix stage reads the input buffer (scale and
 // phase shift fused into that read), middle stages run in a work buffer, and the last
@@ -161,28 +171,30 @@ template <int N>
 constexpr int nt_tma() { return N < 64 ? 64 : (N > 512 ? 512 : N); }
 template <int N>
 constexpr int box_rows() { return N < 256 ? N : 256; }
-template <int N>
-constexpr size_t tma_smem() { return (size_t)(3 * 8 * N + N) * sizeof(double2) + 128 + 2 * sizeof(uint64_t); }
+template <int N, class C>
+constexpr size_t tma_smem() { return (size_t)3 * 128 * N + (size_t)N * sizeof(C) + 128 + 2 * sizeof(uint64_t); }
 // resident CTAs per SM the register budget is built for (shared memory allows this many)
 template <int N>
 constexpr int tma_minb() { return N >= 512 ? 1 : (N == 256 ? 2 : 4); }
 
-template <int N, int AXIS, int DIR, int VARIANT>
+template <int N, int AXIS, int DIR, int VARIANT, class C>
 __global__ void __launch_bounds__(nt_tma<N>(), tma_minb<N>())
-k_yz_tma(const __grid_constant__ CUtensorMap map, TmaArgs a, const double2* __restrict__ tw,
-         const double2* __restrict__ phase, Geom g) {
+k_yz_tma(const __grid_constant__ CUtensorMap map, TmaArgs a, const C* __restrict__ tw,
+         const C* __restrict__ phase, Geom g) {
   constexpr int NT = nt_tma<N>();
   constexpr int BR = box_rows<N>();
   constexpr int NBOX = N / BR;
-  constexpr uint32_t kTileBytes = 8u * N * sizeof(double2);
+  constexpr int TW = tile_cols<C>();
+  constexpr uint32_t kTileBytes = 128u * N;
+  using RT = real_of<C>;
   extern __shared__ unsigned char smraw[];
   __shared__ int s_fail;
-  // 128-byte aligned layout: IN[0], IN[1], W (8N double2 each), twiddles (N), 2 mbarriers
+  // 128-byte aligned layout: IN[0], IN[1], W (TW*N complex each), twiddles (N), 2 mbarriers
   const uint32_t pad = (128u - (smem_u32(smraw) & 127u)) & 127u;
-  double2* in0 = reinterpret_cast<double2*>(smraw + pad);
-  double2* in1 = in0 + 8 * N;
-  double2* W = in1 + 8 * N;
-  double2* s_tw = W + 8 * N;
+  C* in0 = reinterpret_cast<C*>(smraw + pad);
+  C* in1 = in0 + TW * N;
+  C* W = in1 + TW * N;
+  C* s_tw = W + TW * N;
   uint64_t* bars = reinterpret_cast<uint64_t*>(s_tw + N);
   const int tid = threadIdx.x;
   for (int t = tid; t < N; t += NT) s_tw[t] = tw[t];
@@ -199,12 +211,12 @@ k_yz_tma(const __grid_constant__ CUtensorMap map, TmaArgs a, const double2* __re
     const long long q = t / a.ncb;
     const int c = (int)(q % N);
     const int f = a.f_in0 + (int)(q / N);
-    double2* dst = b ? in1 : in0;
+    C* dst = b ? in1 : in0;
     mbar_arrive_expect_tx(&bars[b], kTileBytes);
 #pragma unroll
     for (int k = 0; k < NBOX; ++k) {
-      if constexpr (AXIS == 1) tma_load_4d(dst + k * BR * 8, &map, &bars[b], cb * 16, k * BR, c, f);
-      else tma_load_4d(dst + k * BR * 8, &map, &bars[b], cb * 16, c, k * BR, f);
+      if constexpr (AXIS == 1) tma_load_4d(dst + k * BR * TW, &map, &bars[b], cb * 2 * TW, k * BR, c, f);
+      else tma_load_4d(dst + k * BR * TW, &map, &bars[b], cb * 2 * TW, c, k * BR, f);
     }
   };
   long long t = blockIdx.x;
@@ -226,32 +238,32 @@ k_yz_tma(const __grid_constant__ CUtensorMap map, TmaArgs a, const double2* __re
       return;
     }
     (void)mbar_try_wait(&bars[b], parity);  // acquire the landed tile in every thread
-    const double2* IN = b ? in1 : in0;
+    const C* IN = b ? in1 : in0;
     const int cb = (int)(t % a.ncb);
     const long long q = t / a.ncb;
     const int c = (int)(q % N);
     const int fi = (int)(q / N);
-    const int mx0 = cb * 8;
-    const double sc = a.scale;
+    const int mx0 = cb * TW;
+    const RT sc = (RT)a.scale;
     if constexpr (VARIANT == 0) {
-      double2* outf = a.out + (long long)(a.f_out0 + fi) * g.field;
+      C* outf = static_cast<C*>(a.out) + (long long)(a.f_out0 + fi) * g.field;
       auto src = [&](int s, int e) {
-        const double2 v = IN[e * 8 + s];
-        return sc == 1.0 ? v : cscale(v, sc);
+        const C v = IN[e * TW + s];
+        return sc == RT(1) ? v : cscale(v, sc);
       };
-      auto dst = [&](int s, int e, double2 v) {
+      auto dst = [&](int s, int e, C v) {
         const long long at = AXIS == 1 ? ((long long)c * N + e) * g.pitch : ((long long)e * N + c) * g.pitch;
         outf[at + mx0 + s] = v;
       };
-      tile_fft<N, DIR, NT>(src, W, dst, s_tw, tid);
+      tile_fft<N, DIR, NT, TW>(src, W, dst, s_tw, tid);
     } else {
       static_assert(AXIS == 2, "phase variant is the inverse z pass");
-      double2* out_u = a.out + (long long)(a.f_out0 + 2 * fi) * g.field;
-      double2* out_v = out_u + g.field;
-      auto dst_u = [&](int s, int e, double2 v) { out_u[((long long)e * N + c) * g.pitch + mx0 + s] = v; };
-      auto dst_v = [&](int s, int e, double2 v) { out_v[((long long)e * N + c) * g.pitch + mx0 + s] = v; };
-      auto src_u = [&](int s, int e) { return cscale(IN[e * 8 + s], sc); };
-      tile_fft<N, DIR, NT>(src_u, W, dst_u, s_tw, tid);
+      C* out_u = static_cast<C*>(a.out) + (long long)(a.f_out0 + 2 * fi) * g.field;
+      C* out_v = out_u + g.field;
+      auto dst_u = [&](int s, int e, C v) { out_u[((long long)e * N + c) * g.pitch + mx0 + s] = v; };
+      auto dst_v = [&](int s, int e, C v) { out_v[((long long)e * N + c) * g.pitch + mx0 + s] = v; };
+      auto src_u = [&](int s, int e) { return cscale(IN[e * TW + s], sc); };
+      tile_fft<N, DIR, NT, TW>(src_u, W, dst_u, s_tw, tid);
       __syncthreads();
       const int smy = signed_mode(c, N);
       auto src_v = [&](int s, int e) {
@@ -260,11 +272,11 @@ k_yz_tma(const __grid_constant__ CUtensorMap map, TmaArgs a, const double2* __re
         // past N/2 are padding
         const int mx = mx0 + s;
         const bool anti = mx > 0 && mx < N / 2 && ((c == N / 2) != (e == N / 2));
-        if (mx > N / 2 || anti) return make_double2(0.0, 0.0);
-        const double2 v = cscale(IN[e * 8 + s], sc);
+        if (mx > N / 2 || anti) return czero<C>();
+        const C v = cscale(IN[e * TW + s], sc);
         return cmul(v, __ldg(&phase[mx + smy + signed_mode(e, N) + 3 * N / 2]));
       };
-      tile_fft<N, DIR, NT>(src_v, W, dst_v, s_tw, tid);
+      tile_fft<N, DIR, NT, TW>(src_v, W, dst_v, s_tw, tid);
     }
     __syncthreads();
     if (tid == 0 && t + 2LL * gridDim.x < ntiles) issue(t + 2LL * gridDim.x, b);
@@ -275,20 +287,24 @@ k_yz_tma(const __grid_constant__ CUtensorMap map, TmaArgs a, const double2* __re
 // Packing two Hermitian half spectra A, B (k in [0, N/2]) into Z = A + iB over k in [0, N).
 // At k = 0 and k = N/2 only the real parts enter: that is the Hermitian part of the
 // (y,z)-transformed mx = 0 and mx = N/2 planes, i.e. Re(IDFT) of the reference.
-__device__ __forceinline__ void pack_pair(double2 A, double2 B, int k, int nh, int n, double2* seq_at_k,
-                                          double2* seq_at_mirror) {
+template <class C>
+__device__ __forceinline__ void pack_pair(C A, C B, int k, int nh, int n, C* seq_at_k,
+                                          C* seq_at_mirror) {
   if (k == 0 || k == nh) {
-    *seq_at_k = make_double2(A.x, B.x);
+    *seq_at_k = cmk(A.x, B.x);
   } else {
-    *seq_at_k = make_double2(A.x - B.y, A.y + B.x);
-    *seq_at_mirror = make_double2(A.x + B.y, B.x - A.y);
+    *seq_at_k = cmk(A.x - B.y, A.y + B.x);
+    *seq_at_mirror = cmk(A.x + B.y, B.x - A.y);
   }
 }
 
 // Unpack Z = FFT(a + i b) into the half spectra of a and b at k.
-__device__ __forceinline__ void unpack_pair(double2 Zk, double2 Zm, double2* A, double2* B) {
-  *A = make_double2(0.5 * (Zk.x + Zm.x), 0.5 * (Zk.y - Zm.y));
-  *B = make_double2(0.5 * (Zk.y + Zm.y), -0.5 * (Zk.x - Zm.x));
+template <class C>
+__device__ __forceinline__ void unpack_pair(C Zk, C Zm, C* A, C* B) {
+  using RT = real_of<C>;
+  constexpr RT h = RT(0.5);
+  *A = cmk(h * (Zk.x + Zm.x), h * (Zk.y - Zm.y));
+  *B = cmk(h * (Zk.y + Zm.y), -h * (Zk.x - Zm.x));
 }
 
 template <int NT>
@@ -315,17 +331,18 @@ __device__ __forceinline__ void block_sum_max(double& s, double& m, double* red)
 // Input work fields 0..5 = (U_0, V_0, U_1, V_1, U_2, V_2) [V = shifted grid] after the
 // y and z inverse passes; output work fields 2p, 2p+1 = (P0_p, Ps_p) for the pairs
 // p = 00, 01, 02, 11, 12, 22, columns 0..N/2 (column N/2: per-row Nyquist value).
-template <int N>
+template <int N, class C>
 __global__ void __launch_bounds__(nt_x<N>())
-k_xpass_products(double2* __restrict__ work, const double2* __restrict__ unyq, const double2* __restrict__ phase,
-                 double scale, int nyq_scalar, double* __restrict__ partials, const double2* __restrict__ tw,
+k_xpass_products(C* __restrict__ work, const C* __restrict__ unyq, const C* __restrict__ phase,
+                 double scale, int nyq_scalar, double* __restrict__ partials, const C* __restrict__ tw,
                  Geom g) {
   constexpr int NT = nt_x<N>();
   constexpr int NH = N / 2;
   constexpr int RP = row_pitch(N);
-  extern __shared__ double2 smem[];
-  double2* s_tw = smem;
-  double2* seq = smem + N;  // 6 sequences of pitch RP
+  extern __shared__ __align__(16) unsigned char smraw_x[];
+  C* smem = reinterpret_cast<C*>(smraw_x);
+  C* s_tw = smem;
+  C* seq = smem + N;  // 6 sequences of pitch RP
   __shared__ double red[2 * (NT / 32)];
   const int tid = threadIdx.x;
   load_twiddles<N>(s_tw, tw, tid, NT);
@@ -334,19 +351,19 @@ k_xpass_products(double2* __restrict__ work, const double2* __restrict__ unyq, c
   // pack Z_c = U_c + i V_c
   for (int e = tid; e < 3 * (NH + 1); e += NT) {
     const int c = e / (NH + 1), k = e % (NH + 1);
-    double2 A, B;
+    C A, B;
     if (k == NH && nyq_scalar) {
       // masked state: the mx = N/2 plane holds only (N/2,0,0); after the y/z inverse
       // transforms it is the constant c_N (and phase(N/2,0,0)*c_N on the shifted grid).
-      const double2 cn = cscale(unyq[(long long)c * g.field + NH], scale);
+      const C cn = cscale(unyq[(long long)c * g.field + NH], scale);
       A = cn;
       B = cmul(cn, phase[NH + 3 * N / 2]);
     } else {
       A = work[(long long)(2 * c) * g.field + rbase + k];
       B = work[(long long)(2 * c + 1) * g.field + rbase + k];
     }
-    double2* sq = seq + c * RP;
-    double2 zk, zm;
+    C* sq = seq + c * RP;
+    C zk, zm;
     pack_pair(A, B, k, NH, N, &zk, &zm);
     sq[k + (k >> 3)] = zk;
     if (k != 0 && k != NH) sq[(N - k) + ((N - k) >> 3)] = zm;
@@ -356,16 +373,17 @@ k_xpass_products(double2* __restrict__ work, const double2* __restrict__ unyq, c
   double esum = 0.0, vmax2 = 0.0;
   for (int x = tid; x < N; x += NT) {
     const int p = x + (x >> 3);
-    const double2 z0 = seq[p], z1 = seq[RP + p], z2 = seq[2 * RP + p];
-    const double s2 = z0.x * z0.x + z1.x * z1.x + z2.x * z2.x;
+    const C z0 = seq[p], z1 = seq[RP + p], z2 = seq[2 * RP + p];
+    const double a0 = z0.x, a1 = z1.x, a2 = z2.x;
+    const double s2 = a0 * a0 + a1 * a1 + a2 * a2;
     esum += 0.5 * s2;
     vmax2 = fmax(vmax2, s2);
-    seq[0 * RP + p] = make_double2(z0.x * z0.x, z0.y * z0.y);
-    seq[1 * RP + p] = make_double2(z0.x * z1.x, z0.y * z1.y);
-    seq[2 * RP + p] = make_double2(z0.x * z2.x, z0.y * z2.y);
-    seq[3 * RP + p] = make_double2(z1.x * z1.x, z1.y * z1.y);
-    seq[4 * RP + p] = make_double2(z1.x * z2.x, z1.y * z2.y);
-    seq[5 * RP + p] = make_double2(z2.x * z2.x, z2.y * z2.y);
+    seq[0 * RP + p] = cmk(z0.x * z0.x, z0.y * z0.y);
+    seq[1 * RP + p] = cmk(z0.x * z1.x, z0.y * z1.y);
+    seq[2 * RP + p] = cmk(z0.x * z2.x, z0.y * z2.y);
+    seq[3 * RP + p] = cmk(z1.x * z1.x, z1.y * z1.y);
+    seq[4 * RP + p] = cmk(z1.x * z2.x, z1.y * z2.y);
+    seq[5 * RP + p] = cmk(z2.x * z2.x, z2.y * z2.y);
   }
   if (partials != nullptr) {
     block_sum_max<NT>(esum, vmax2, red);
@@ -379,9 +397,9 @@ k_xpass_products(double2* __restrict__ work, const double2* __restrict__ unyq, c
   for (int e = tid; e < 6 * (NH + 1); e += NT) {
     const int pr = e / (NH + 1), k = e % (NH + 1);
     const int km = (N - k) % N;
-    const double2 Zk = seq[pr * RP + k + (k >> 3)];
-    const double2 Zm = seq[pr * RP + km + (km >> 3)];
-    double2 A, B;
+    const C Zk = seq[pr * RP + k + (k >> 3)];
+    const C Zm = seq[pr * RP + km + (km >> 3)];
+    C A, B;
     unpack_pair(Zk, Zm, &A, &B);
     work[(long long)(2 * pr) * g.field + rbase + k] = A;
     work[(long long)(2 * pr + 1) * g.field + rbase + k] = B;
@@ -402,7 +420,7 @@ k_xpass_products(double2* __restrict__ work, const double2* __restrict__ unyq, c
 //                     with the mirror fetched from the partner lane by a shuffle, and
 //                     128-byte stores straight to HBM
 // The (N/2,0,0) sums of the 12 product planes accumulate in registers per CTA.
-template <int N>
+template <int N, class C>
 struct XP {
   static constexpr int M = N / 16;                 // stage-B radix
   static constexpr bool PAIR = (M == 32);          // radix 32 as two radix-16 halves + shuffle
@@ -410,36 +428,43 @@ struct XP {
   static constexpr int ROWS = (N == 256) ? 2 : 1;  // rows per iteration (192 threads busy)
   static constexpr int SP = N + N / 16;            // padded sequence (one slot per 16)
   static constexpr int NT = 192;
-  static constexpr int ROWIN = 6 * (NH + 1);
+  // resident CTAs per SM the register budget is built for: the FP32 rows are half the
+  // shared memory, so three CTAs fit where FP64 fits two
+  static constexpr int MINB = sizeof(C) == 8 ? 3 : 2;
+  // staged row of one field: NH + 1 values rounded up to 16 bytes (the bulk-copy unit)
+  static constexpr int RS = (int)(((NH + 1) * sizeof(C) + 15) / 16 * 16 / sizeof(C));
+  static constexpr int ROWIN = 6 * RS;
   static constexpr int STG = (ROWIN > 3 * SP ? ROWIN : 3 * SP);
-  static constexpr uint32_t kRowBytes = (NH + 1) * sizeof(double2);
-  static constexpr size_t smem = (size_t)(2 * ROWS * STG + ROWS * 6 * SP + N) * sizeof(double2) + 128 +
+  static constexpr uint32_t kRowBytes = RS * sizeof(C);
+  static constexpr size_t smem = (size_t)(2 * ROWS * STG + ROWS * 6 * SP + N) * sizeof(C) + 128 +
                                  2 * sizeof(uint64_t);
 };
 
 __device__ __forceinline__ int pp16(int e) { return e + (e >> 4); }
 
-__device__ __forceinline__ double2 shfl2(double2 v, int src) {
-  return make_double2(__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src));
+template <class C>
+__device__ __forceinline__ C shfl2(C v, int src) {
+  return cmk(__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src));
 }
-__device__ __forceinline__ double2 shfl2_xor(double2 v, int m) {
-  return make_double2(__shfl_xor_sync(0xffffffffu, v.x, m), __shfl_xor_sync(0xffffffffu, v.y, m));
+template <class C>
+__device__ __forceinline__ C shfl2_xor(C v, int m) {
+  return cmk(__shfl_xor_sync(0xffffffffu, v.x, m), __shfl_xor_sync(0xffffffffu, v.y, m));
 }
 
-template <int N>
-__global__ void __launch_bounds__(192, 2)
-k_xpass2(double2* __restrict__ work, const double2* __restrict__ unyq, const double2* __restrict__ phase,
-         double scale, int nyq_scalar, double* __restrict__ nyq_part, const double2* __restrict__ tw2_g, Geom g,
+template <int N, class C>
+__global__ void __launch_bounds__(192, XP<N, C>::MINB)
+k_xpass2(C* __restrict__ work, const C* __restrict__ unyq, const C* __restrict__ phase,
+         double scale, int nyq_scalar, double* __restrict__ nyq_part, const C* __restrict__ tw2_g, Geom g,
          int* err) {
-  using X = XP<N>;
-  constexpr int M = X::M, NH = X::NH, ROWS = X::ROWS, SP = X::SP, STG = X::STG;
+  using X = XP<N, C>;
+  constexpr int M = X::M, NH = X::NH, ROWS = X::ROWS, SP = X::SP, STG = X::STG, RS = X::RS;
   extern __shared__ unsigned char smraw[];
   __shared__ int s_fail;
   __shared__ double s_nyq[2][12];
   const uint32_t pad = (128u - (smem_u32(smraw) & 127u)) & 127u;
-  double2* stg = reinterpret_cast<double2*>(smraw + pad);  // [2][ROWS][STG]
-  double2* W = stg + 2 * ROWS * STG;                       // [ROWS][6][SP]
-  double2* tw2 = W + ROWS * 6 * SP;                        // [M][16]: W_N^(r*j)
+  C* stg = reinterpret_cast<C*>(smraw + pad);  // [2][ROWS][STG]
+  C* W = stg + 2 * ROWS * STG;                       // [ROWS][6][SP]
+  C* tw2 = W + ROWS * 6 * SP;                        // [M][16]: W_N^(r*j)
   uint64_t* bars = reinterpret_cast<uint64_t*>(tw2 + N);
   const int tid = threadIdx.x;
   for (int t = tid; t < N; t += 192) tw2[t] = tw2_g[t];
@@ -458,7 +483,7 @@ k_xpass2(double2* __restrict__ work, const double2* __restrict__ unyq, const dou
       const long long row = it * ROWS + r;
 #pragma unroll
       for (int f = 0; f < 6; ++f)
-        bulk_load(stg + (b * ROWS + r) * STG + f * (NH + 1), work + (long long)f * g.field + row * g.pitch,
+        bulk_load(stg + (b * ROWS + r) * STG + f * RS, work + (long long)f * g.field + row * g.pitch,
                   X::kRowBytes, &bars[b]);
     }
   };
@@ -481,25 +506,25 @@ k_xpass2(double2* __restrict__ work, const double2* __restrict__ unyq, const dou
       return;
     }
     (void)mbar_try_wait(&bars[b], parity);
-    double2* S = stg + b * ROWS * STG;
+    C* S = stg + b * ROWS * STG;
 
     // ---- inverse stage A: (r, c, t), packing fused into the loads
     if (tid < ROWS * 3 * M) {
       const int t = tid % M, c = (tid / M) % 3, r = tid / (3 * M);
-      const double2* Ur = S + r * STG + (2 * c) * (NH + 1);
-      const double2* Vr = Ur + (NH + 1);
-      double2 v[16];
+      const C* Ur = S + r * STG + (2 * c) * RS;
+      const C* Vr = Ur + RS;
+      C v[16];
 #pragma unroll
       for (int q = 0; q < 16; ++q) {
         const int x = t + M * q;
-        double2 z;
+        C z;
         if (x == 0) {
-          z = make_double2(Ur[0].x, Vr[0].x);
+          z = cmk(Ur[0].x, Vr[0].x);
         } else if (x < NH) {
-          const double2 U = Ur[x], V = Vr[x];
-          z = make_double2(U.x - V.y, U.y + V.x);
+          const C U = Ur[x], V = Vr[x];
+          z = cmk(U.x - V.y, U.y + V.x);
         } else if (x == NH) {
-          double2 U, V;
+          C U, V;
           if (nyq_scalar) {
             U = cscale(unyq[(long long)c * g.field + NH], scale);
             V = cmul(U, phase[NH + 3 * N / 2]);
@@ -507,15 +532,15 @@ k_xpass2(double2* __restrict__ work, const double2* __restrict__ unyq, const dou
             U = Ur[NH];
             V = Vr[NH];
           }
-          z = make_double2(U.x, V.x);
+          z = cmk(U.x, V.x);
         } else {
-          const double2 U = Ur[N - x], V = Vr[N - x];
-          z = make_double2(U.x + V.y, V.x - U.y);
+          const C U = Ur[N - x], V = Vr[N - x];
+          z = cmk(U.x + V.y, V.x - U.y);
         }
         v[q] = z;
       }
       dft16<+1>(v);
-      double2* Wc = W + (r * 6 + c) * SP;
+      C* Wc = W + (r * 6 + c) * SP;
 #pragma unroll
       for (int q = 0; q < 16; ++q) Wc[pp16(16 * t + q)] = v[q];
     }
@@ -525,8 +550,8 @@ k_xpass2(double2* __restrict__ work, const double2* __restrict__ unyq, const dou
     if constexpr (X::PAIR) {
       if (tid < 96) {
         const int lane = tid & 31, c = tid >> 5, j = lane & 15, h = lane >> 4;
-        const double2* Wc = W + c * SP;
-        double2 v[16];
+        const C* Wc = W + c * SP;
+        C v[16];
 #pragma unroll
         for (int i = 0; i < 16; ++i) {
           const int rr = 2 * i + h;
@@ -537,23 +562,23 @@ k_xpass2(double2* __restrict__ work, const double2* __restrict__ unyq, const dou
 #pragma unroll
           for (int q = 1; q < 16; ++q) v[q] = cmulc(v[q], tw2[16 * 16 + q]);  // conj W32^q
         }
-        double2* Zc = S + c * SP;
+        C* Zc = S + c * SP;
 #pragma unroll
         for (int q = 0; q < 16; ++q) {
-          const double2 o = shfl2_xor(v[q], 16);
-          const double2 z = h ? csub(o, v[q]) : cadd(v[q], o);
+          const C o = shfl2_xor(v[q], 16);
+          const C z = h ? csub(o, v[q]) : cadd(v[q], o);
           Zc[pp16(j + 16 * (q + 16 * h))] = z;
         }
       }
     } else {
       if (tid < ROWS * 3 * 16) {
         const int j = tid & 15, c = (tid >> 4) % 3, r = tid / 48;
-        const double2* Wc = W + (r * 6 + c) * SP;
-        double2 v[16];
+        const C* Wc = W + (r * 6 + c) * SP;
+        C v[16];
 #pragma unroll
         for (int q = 0; q < 16; ++q) v[q] = q == 0 ? Wc[pp16(j)] : cmulc(Wc[pp16(j + 16 * q)], tw2[q * 16 + j]);
         dft16<+1>(v);
-        double2* Zc = S + r * STG + c * SP;
+        C* Zc = S + r * STG + c * SP;
 #pragma unroll
         for (int q = 0; q < 16; ++q) Zc[pp16(j + 16 * q)] = v[q];
       }
@@ -565,17 +590,17 @@ k_xpass2(double2* __restrict__ work, const double2* __restrict__ unyq, const dou
       const int t = tid % M, ab = (tid / M) % 6, r = tid / (6 * M);
       // pairs 00 01 02 11 12 22
       const int ca = (ab >= 3) + (ab >= 5), cb = ab < 3 ? ab : (ab < 5 ? ab - 2 : 2);
-      const double2* Za = S + r * STG + ca * SP;
-      const double2* Zb = S + r * STG + cb * SP;
-      double2 v[16];
+      const C* Za = S + r * STG + ca * SP;
+      const C* Zb = S + r * STG + cb * SP;
+      C v[16];
 #pragma unroll
       for (int q = 0; q < 16; ++q) {
         const int x = pp16(t + M * q);
-        const double2 za = Za[x], zb = Zb[x];
-        v[q] = make_double2(za.x * zb.x, za.y * zb.y);
+        const C za = Za[x], zb = Zb[x];
+        v[q] = cmk(za.x * zb.x, za.y * zb.y);
       }
       dft16<-1>(v);
-      double2* Wp = W + (r * 6 + ab) * SP;
+      C* Wp = W + (r * 6 + ab) * SP;
 #pragma unroll
       for (int q = 0; q < 16; ++q) Wp[pp16(16 * t + q)] = v[q];
     }
@@ -584,8 +609,8 @@ k_xpass2(double2* __restrict__ work, const double2* __restrict__ unyq, const dou
     // ---- forward stage B, r2c unpack through the partner lane, stores to HBM
     if constexpr (X::PAIR) {
       const int lane = tid & 31, ab = tid >> 5, j = lane & 15, h = lane >> 4;
-      const double2* Wp = W + ab * SP;
-      double2 v[16];
+      const C* Wp = W + ab * SP;
+      C v[16];
 #pragma unroll
       for (int i = 0; i < 16; ++i) {
         const int rr = 2 * i + h;
@@ -598,21 +623,21 @@ k_xpass2(double2* __restrict__ work, const double2* __restrict__ unyq, const dou
       }
 #pragma unroll
       for (int q = 0; q < 16; ++q) {
-        const double2 o = shfl2_xor(v[q], 16);
+        const C o = shfl2_xor(v[q], 16);
         v[q] = h ? csub(o, v[q]) : cadd(v[q], o);  // X(j + 16 (q + 16 h))
       }
       const int partner = ((16 - j) & 15) + 16 * (1 - h);
       const long long row = it;
-      double2* o0 = work + (long long)(2 * ab) * g.field + row * g.pitch;
-      double2* o1 = o0 + g.field;
+      C* o0 = work + (long long)(2 * ab) * g.field + row * g.pitch;
+      C* o1 = o0 + g.field;
 #pragma unroll
       for (int i = 0; i < 16; ++i) {
-        const double2 send = j == 0 ? v[(16 - i) & 15] : v[15 - i];
-        const double2 recv = shfl2(send, partner);
-        const double2 zm = (j == 0 && i == 0) ? v[0] : recv;
+        const C send = j == 0 ? v[(16 - i) & 15] : v[15 - i];
+        const C recv = shfl2(send, partner);
+        const C zm = (j == 0 && i == 0) ? v[0] : recv;
         const int kk = j + 16 * (16 * h + i);
         if (kk <= NH) {
-          double2 A, B;
+          C A, B;
           unpack_pair(v[i], zm, &A, &B);
           o0[kk] = A;
           o1[kk] = B;
@@ -624,23 +649,23 @@ k_xpass2(double2* __restrict__ work, const double2* __restrict__ unyq, const dou
       }
     } else {
       const int j = tid & 15, sq = tid >> 4, r = sq / 6, ab = sq % 6;
-      const double2* Wp = W + (r * 6 + ab) * SP;
-      double2 v[16];
+      const C* Wp = W + (r * 6 + ab) * SP;
+      C v[16];
 #pragma unroll
       for (int q = 0; q < 16; ++q) v[q] = q == 0 ? Wp[pp16(j)] : cmul(Wp[pp16(j + 16 * q)], tw2[q * 16 + j]);
       dft16<-1>(v);
       const int lane = tid & 31;
       const int partner = (lane & 16) + ((16 - j) & 15);
       const long long row = it * ROWS + r;
-      double2* o0 = work + (long long)(2 * ab) * g.field + row * g.pitch;
-      double2* o1 = o0 + g.field;
+      C* o0 = work + (long long)(2 * ab) * g.field + row * g.pitch;
+      C* o1 = o0 + g.field;
 #pragma unroll
       for (int q = 0; q < 16; ++q) {
-        const double2 recv = shfl2(v[15 - q], partner);
-        const double2 zm = j == 0 ? v[(16 - q) & 15] : recv;
+        const C recv = shfl2(v[15 - q], partner);
+        const C zm = j == 0 ? v[(16 - q) & 15] : recv;
         const int kk = j + 16 * q;
         if (kk <= NH) {
-          double2 A, B;
+          C A, B;
           unpack_pair(v[q], zm, &A, &B);
           o0[kk] = A;
           o1[kk] = B;
@@ -675,10 +700,11 @@ k_xpass2(double2* __restrict__ work, const double2* __restrict__ unyq, const dou
 // Nyquist-plane sums: column N/2 of each of the 12 product fields summed over all rows
 // (the (N/2,0,0) output of the y/z forward transforms is the plain sum of the plane).
 // grid 12, fixed summation order.
-__global__ void __launch_bounds__(256) k_nyq_reduce(const double2* __restrict__ work, double* __restrict__ sums,
+template <class C>
+__global__ void __launch_bounds__(256) k_nyq_reduce(const C* __restrict__ work, double* __restrict__ sums,
                                                     Geom g) {
   __shared__ double red[256];
-  const double2* f = work + (long long)blockIdx.x * g.field + g.nh;
+  const C* f = work + (long long)blockIdx.x * g.field + g.nh;
   const long long rows = (long long)g.n * g.n;
   double s = 0.0;
   for (long long r = threadIdx.x; r < rows; r += 256) s += f[r * g.pitch].x;
@@ -694,48 +720,54 @@ __global__ void __launch_bounds__(256) k_nyq_reduce(const double2* __restrict__ 
 // ------------------------------------------------------------------------------------
 // P5 sweep: per mode, the reference's accumulate (:926-936), add_viscous_project
 // (:955-974), RK stage update (:994-1033) and project_truncate (:825-844).
+template <class C>
 struct ModeIn {
-  double2 p0[6];
-  double2 ps[6];
+  C p0[6];
+  C ps[6];
 };
 
-__device__ __forceinline__ double2 minus_i_k(double2 a, int k) {
-  const double rk = (double)k;
-  return make_double2(rk * a.y, -rk * a.x);
+template <class C>
+__device__ __forceinline__ C minus_i_k(C a, int k) {
+  const real_of<C> rk = (real_of<C>)k;
+  return cmk(rk * a.y, -rk * a.x);
 }
 
 // Dealiased product value of one pair at one mode (accumulate lambda, :928-931).
-__device__ __forceinline__ double2 pair_value(double2 p0, double2 ps, double2 phase, bool keep, int dealias) {
-  double2 value = dealias ? cscale(cadd(p0, cmulc(ps, phase)), 0.5) : p0;
-  if (!keep) value = make_double2(0.0, 0.0);
+template <class C>
+__device__ __forceinline__ C pair_value(C p0, C ps, C phase, bool keep, int dealias) {
+  C value = dealias ? cscale(cadd(p0, cmulc(ps, phase)), 0.5) : p0;
+  if (!keep) value = czero<C>();
   return value;
 }
 
 // Viscous term, Leray projection and mask (:955-974), then the RK stage update and the
 // projection of u (:994-1039) -- or the RHS itself in modes 1 and 2.
-__device__ __forceinline__ void finish_mode(double2 r[3], int ix, int iy, int iz, int n, double2 uu[3], double2 gg[3],
-                                            bool load_g, double2 rr[3], const SweepArgs& a);
+template <class C>
+__device__ __forceinline__ void finish_mode(C r[3], int ix, int iy, int iz, int n, C uu[3], C gg[3],
+                                            bool load_g, C rr[3], const SweepArgs& a);
 
-__device__ __forceinline__ void sweep_mode(const ModeIn& in, int ix, int iy, int iz, int n, double2 phase,
-                                           double2 uu[3], double2 gg[3], bool load_g, double2 rr[3],
+template <class C>
+__device__ __forceinline__ void sweep_mode(const ModeIn<C>& in, int ix, int iy, int iz, int n, C phase,
+                                           C uu[3], C gg[3], bool load_g, C rr[3],
                                            const SweepArgs& a) {
   const int m2 = ix * ix + iy * iy + iz * iz;
   const bool keep = 4LL * m2 <= (long long)n * n;
   const int kv[3] = {ix, iy, iz};
-  double2 r[3] = {make_double2(0, 0), make_double2(0, 0), make_double2(0, 0)};
+  C r[3] = {czero<C>(), czero<C>(), czero<C>()};
   const int pa[6] = {0, 0, 0, 1, 1, 2};
   const int pb[6] = {0, 1, 2, 1, 2, 2};
 #pragma unroll
   for (int p = 0; p < 6; ++p) {
-    const double2 value = pair_value(in.p0[p], in.ps[p], phase, keep, a.dealias);
+    const C value = pair_value(in.p0[p], in.ps[p], phase, keep, a.dealias);
     r[pa[p]] = cadd(r[pa[p]], minus_i_k(value, kv[pb[p]]));
     if (pa[p] != pb[p]) r[pb[p]] = cadd(r[pb[p]], minus_i_k(value, kv[pa[p]]));
   }
   finish_mode(r, ix, iy, iz, n, uu, gg, load_g, rr, a);
 }
 
-__device__ __forceinline__ void finish_mode(double2 r[3], int ix, int iy, int iz, int n, double2 uu[3], double2 gg[3],
-                                            bool load_g, double2 rr[3], const SweepArgs& a) {
+template <class C>
+__device__ __forceinline__ void finish_mode(C r[3], int ix, int iy, int iz, int n, C uu[3], C gg[3],
+                                            bool load_g, C rr[3], const SweepArgs& a) {
   const int m2 = ix * ix + iy * iy + iz * iz;
   const bool keep = 4LL * m2 <= (long long)n * n;
   const double k2 = (double)m2;
@@ -745,16 +777,18 @@ __device__ __forceinline__ void finish_mode(double2 r[3], int ix, int iy, int iz
     rr[2] = r[2];
     return;
   }
+  if (!a.visc_if) {
 #pragma unroll
-  for (int c = 0; c < 3; ++c) r[c] = csub(r[c], cscale(uu[c], a.nu * k2));
+    for (int c = 0; c < 3; ++c) r[c] = csub(r[c], cscale(uu[c], a.nu * k2));
+  }
   if (k2 > 0.0 && keep) {
-    const double2 dot = cadd(cadd(cscale(r[0], (double)ix), cscale(r[1], (double)iy)), cscale(r[2], (double)iz));
-    const double2 factor = cscale(dot, 1.0 / k2);
+    const C dot = cadd(cadd(cscale(r[0], (double)ix), cscale(r[1], (double)iy)), cscale(r[2], (double)iz));
+    const C factor = cscale(dot, 1.0 / k2);
     r[0] = csub(r[0], cscale(factor, (double)ix));
     r[1] = csub(r[1], cscale(factor, (double)iy));
     r[2] = csub(r[2], cscale(factor, (double)iz));
   } else {
-    r[0] = r[1] = r[2] = make_double2(0.0, 0.0);
+    r[0] = r[1] = r[2] = czero<C>();
   }
   if (a.mode == 1) {
     rr[0] = r[0];
@@ -767,21 +801,30 @@ __device__ __forceinline__ void finish_mode(double2 r[3], int ix, int iy, int iz
     gg[c] = load_g ? cadd(cscale(gg[c], a.ga), r[c]) : r[c];
     uu[c] = cadd(uu[c], cscale(gg[c], a.ub));
   }
+  if (a.visc_if) {
+    // integrating factor to the next stage time, exponent in FP64 for either precision
+    const double f = exp(-a.nu * k2 * a.if_tau);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      uu[c] = cscale(uu[c], f);
+      gg[c] = cscale(gg[c], f);
+    }
+  }
   if (k2 > 0.0 && keep) {
-    const double2 dot = cadd(cadd(cscale(uu[0], (double)ix), cscale(uu[1], (double)iy)), cscale(uu[2], (double)iz));
-    const double2 factor = cscale(dot, 1.0 / k2);
+    const C dot = cadd(cadd(cscale(uu[0], (double)ix), cscale(uu[1], (double)iy)), cscale(uu[2], (double)iz));
+    const C factor = cscale(dot, 1.0 / k2);
     uu[0] = csub(uu[0], cscale(factor, (double)ix));
     uu[1] = csub(uu[1], cscale(factor, (double)iy));
     uu[2] = csub(uu[2], cscale(factor, (double)iz));
   } else {
-    uu[0] = uu[1] = uu[2] = make_double2(0.0, 0.0);
+    uu[0] = uu[1] = uu[2] = czero<C>();
   }
 }
 
-template <int N>
+template <int N, class C>
 __global__ void __launch_bounds__(256)
-k_sweep(const double2* __restrict__ work, double2* __restrict__ u, double2* __restrict__ gbuf,
-        double2* __restrict__ rhs, const double* __restrict__ nyq_part, int nparts, const double2* __restrict__ phase,
+k_sweep(const C* __restrict__ work, C* __restrict__ u, C* __restrict__ gbuf,
+        C* __restrict__ rhs, const double* __restrict__ nyq_part, int nparts, const C* __restrict__ phase,
         SweepArgs a, Geom g) {
   constexpr int NH = N / 2;
   const long long e = (long long)blockIdx.x * 256 + threadIdx.x;
@@ -793,17 +836,17 @@ k_sweep(const double2* __restrict__ work, double2* __restrict__ u, double2* __re
     const int my = signed_mode((int)(row % N), N);
     const int mz = signed_mode((int)(row / N), N);
     const long long idx = row * g.pitch + mx;
-    ModeIn in;
+    ModeIn<C> in;
 #pragma unroll
     for (int p = 0; p < 6; ++p) {
       in.p0[p] = work[(long long)(2 * p) * g.field + idx];
       in.ps[p] = work[(long long)(2 * p + 1) * g.field + idx];
     }
-    double2 uu[3], gg[3], rr[3];
+    C uu[3], gg[3], rr[3];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       uu[c] = u[(long long)c * g.field + idx];
-      gg[c] = load_g ? gbuf[(long long)c * g.field + idx] : make_double2(0, 0);
+      gg[c] = load_g ? gbuf[(long long)c * g.field + idx] : czero<C>();
     }
     sweep_mode(in, mx, my, mz, N, phase[mx + my + mz + 3 * N / 2], uu, gg, load_g, rr, a);
     if (a.mode != 0) {
@@ -820,7 +863,7 @@ k_sweep(const double2* __restrict__ work, double2* __restrict__ u, double2* __re
     // masked RHS, g and projected u are zero there.  Row 0 is written below.
     if (mx == 0 && row != 0) {
       const long long inq = row * g.pitch + NH;
-      const double2 zero = make_double2(0.0, 0.0);
+      const C zero = czero<C>();
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
         if (a.mode != 0) {
@@ -845,18 +888,18 @@ k_sweep(const double2* __restrict__ work, double2* __restrict__ u, double2* __re
       part[f] = acc;
     }
   if (threadIdx.x == 0) {
-    ModeIn in;
+    ModeIn<C> in;
 #pragma unroll
     for (int p = 0; p < 6; ++p) {
-      in.p0[p] = make_double2(part[2 * p], 0.0);
-      in.ps[p] = make_double2(part[2 * p + 1], 0.0);
+      in.p0[p] = cmk((real_of<C>)part[2 * p], real_of<C>(0));
+      in.ps[p] = cmk((real_of<C>)part[2 * p + 1], real_of<C>(0));
     }
     const long long idx = NH;
-    double2 uu[3], gg[3], rr[3];
+    C uu[3], gg[3], rr[3];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       uu[c] = u[(long long)c * g.field + idx];
-      gg[c] = load_g ? gbuf[(long long)c * g.field + idx] : make_double2(0, 0);
+      gg[c] = load_g ? gbuf[(long long)c * g.field + idx] : czero<C>();
     }
     sweep_mode(in, NH, 0, 0, N, phase[NH + 3 * N / 2], uu, gg, load_g, rr, a);
     if (a.mode != 0) {
@@ -878,10 +921,10 @@ k_sweep(const double2* __restrict__ work, double2* __restrict__ u, double2* __re
 // The self-conjugate mode (N/2, 0, 0) for the fused P5 path: one warp sums the x pass's
 // per-CTA plane sums in a fixed order and runs the sweep on that single mode (column N/2
 // of row 0, which no P5 tile touches).
-template <int N>
-__global__ void __launch_bounds__(32) k_nyq_mode(double2* __restrict__ u, double2* __restrict__ gbuf,
-                                                 double2* __restrict__ rhs, const double* __restrict__ nyq_part,
-                                                 int nparts, const double2* __restrict__ phase, SweepArgs a, Geom g) {
+template <int N, class C>
+__global__ void __launch_bounds__(32) k_nyq_mode(C* __restrict__ u, C* __restrict__ gbuf,
+                                                 C* __restrict__ rhs, const double* __restrict__ nyq_part,
+                                                 int nparts, const C* __restrict__ phase, SweepArgs a, Geom g) {
   constexpr int NH = N / 2;
   const int tid = threadIdx.x;
   const bool load_g = a.stage > 0;
@@ -895,17 +938,17 @@ __global__ void __launch_bounds__(32) k_nyq_mode(double2* __restrict__ u, double
     part[f] = acc;
   }
   if (tid != 0) return;
-  ModeIn in;
+  ModeIn<C> in;
 #pragma unroll
   for (int p = 0; p < 6; ++p) {
-    in.p0[p] = make_double2(part[2 * p], 0.0);
-    in.ps[p] = make_double2(part[2 * p + 1], 0.0);
+    in.p0[p] = cmk((real_of<C>)part[2 * p], real_of<C>(0));
+    in.ps[p] = cmk((real_of<C>)part[2 * p + 1], real_of<C>(0));
   }
-  double2 uu[3], gg[3], rr[3];
+  C uu[3], gg[3], rr[3];
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
     uu[c] = u[(long long)c * g.field + NH];
-    gg[c] = load_g ? gbuf[(long long)c * g.field + NH] : make_double2(0, 0);
+    gg[c] = load_g ? gbuf[(long long)c * g.field + NH] : czero<C>();
   }
   sweep_mode(in, NH, 0, 0, N, phase[NH + 3 * N / 2], uu, gg, load_g, rr, a);
 #pragma unroll
@@ -922,44 +965,46 @@ __global__ void __launch_bounds__(32) k_nyq_mode(double2* __restrict__ u, double
 // ------------------------------------------------------------------------------------
 // P5 fused (N = 128, 256, 512): forward z pass of the 12 product fields and the whole
 // k-space sweep in one persistent kernel, so the transformed products never return to HBM.
-// A tile is (8 columns mx, one my, all mz); its 12 field tiles arrive one after another
+// A tile is (TW columns mx, one my, all mz); its 12 field tiles arrive one after another
 // through TMA (double-buffered).  The z FFT leaves each thread 8 modes in registers:
 //   P0 field of pair p -> parked in tensor memory;
 //   Ps field of pair p -> combined with the parked P0 into the dealiased value, whose -i k
 //                          contributions accumulate into r_x, r_y, r_z in tensor memory, in
 //                          the reference's order (pairs 00 01 02 11 12 22);
 //   after the 12th      -> viscous term, Leray projection, RK3 update and projection of u.
-// Tensor memory per thread: 4 x 32 columns (P0, r_x, r_y, r_z: 8 complex each).
+// Tensor memory per thread: 4 blocks of CW columns (P0, r_x, r_y, r_z).
 template <int N>
 constexpr uint32_t p5_cols() { return N == 512 ? 512u : (N == 256 ? 256u : 128u); }
 template <int N>
 constexpr int nt_p5() { return nt_tma<N>(); }
 
-template <int N>
+template <int N, class C>
 __global__ void __launch_bounds__(nt_p5<N>(), tma_minb<N>())
-k_p5(const __grid_constant__ CUtensorMap map, double2* __restrict__ u, double2* __restrict__ gbuf,
-     double2* __restrict__ rhs, const double* __restrict__ nyq_part, int nparts, const double2* __restrict__ tw,
-     const double2* __restrict__ phase, SweepArgs a, int ncb, Geom g, int* err) {
+k_p5(const __grid_constant__ CUtensorMap map, C* __restrict__ u, C* __restrict__ gbuf,
+     C* __restrict__ rhs, const double* __restrict__ nyq_part, int nparts, const C* __restrict__ tw,
+     const C* __restrict__ phase, SweepArgs a, int ncb, Geom g, int* err) {
   constexpr int NT = nt_p5<N>();
   constexpr int BR = box_rows<N>();
   constexpr int NBOX = N / BR;
   constexpr int NH = N / 2;
-  constexpr uint32_t kTileBytes = 8u * N * sizeof(double2);
+  constexpr int TW = tile_cols<C>();
+  constexpr uint32_t kTileBytes = 128u * N;
   constexpr uint32_t COLS = p5_cols<N>();
-  using RO = RegOut<N, NT>;
-  constexpr int MPT = RO::KB * RO::R;  // modes per thread
-  constexpr int CW = 4 * MPT;          // tensor-memory words per field of modes
+  using RO = LastStage<N, NT, TW>;
+  constexpr int WPC = tmem_words<C>();  // tensor-memory words per complex value
+  constexpr int MPT = RO::KB * RO::R;    // modes per thread
+  constexpr int CW = WPC * MPT;          // tensor-memory words per field of modes
   static_assert(RO::R == 4 || RO::R == 8, "last radix moves through tensor memory");
   static_assert((NT / 32 + 3) / 4 * 4 * CW <= (int)COLS, "tensor memory budget");
-  static_assert((8 * (N / RO::R)) % NT == 0, "every thread owns whole butterflies");
+  static_assert((TW * (N / RO::R)) % NT == 0, "every thread owns whole butterflies");
   extern __shared__ unsigned char smraw[];
   __shared__ int s_fail;
   __shared__ uint32_t s_tmem;
   const uint32_t pad = (128u - (smem_u32(smraw) & 127u)) & 127u;
-  double2* in0 = reinterpret_cast<double2*>(smraw + pad);
-  double2* in1 = in0 + 8 * N;
-  double2* W = in1 + 8 * N;
-  double2* s_tw = W + 8 * N;
+  C* in0 = reinterpret_cast<C*>(smraw + pad);
+  C* in1 = in0 + TW * N;
+  C* W = in1 + TW * N;
+  C* s_tw = W + TW * N;
   uint64_t* bars = reinterpret_cast<uint64_t*>(s_tw + N);
   const int tid = threadIdx.x, warp = tid >> 5;
   for (int t = tid; t < N; t += NT) s_tw[t] = tw[t];
@@ -986,10 +1031,10 @@ k_p5(const __grid_constant__ CUtensorMap map, double2* __restrict__ u, double2* 
     const long long t = blockIdx.x + (ul / 12) * gridDim.x;
     const int f = (int)(ul % 12);
     const int cb = (int)(t % ncb), my = (int)(t / ncb);
-    double2* dst = b ? in1 : in0;
+    C* dst = b ? in1 : in0;
     mbar_arrive_expect_tx(&bars[b], kTileBytes);
 #pragma unroll
-    for (int k = 0; k < NBOX; ++k) tma_load_4d(dst + k * BR * 8, &map, &bars[b], cb * 16, my, k * BR, f);
+    for (int k = 0; k < NBOX; ++k) tma_load_4d(dst + k * BR * TW, &map, &bars[b], cb * 2 * TW, my, k * BR, f);
   };
   if (tid == 0) {
     if (nunits > 0) issue(0, 0);
@@ -1009,21 +1054,21 @@ k_p5(const __grid_constant__ CUtensorMap map, double2* __restrict__ u, double2* 
       return;
     }
     (void)mbar_try_wait(&bars[b], parity);
-    const double2* IN = b ? in1 : in0;
+    const C* IN = b ? in1 : in0;
     const long long t = blockIdx.x + (ul / 12) * gridDim.x;
     const int f = (int)(ul % 12);
     const int cb = (int)(t % ncb), my = (int)(t / ncb);
-    const int mx0 = cb * 8;
+    const int mx0 = cb * TW;
     // Each radix butterfly of the last stage hands its R modes to the sink: column
-    // s = b & 7 (b = tid + i*NT), z index (j/NS)*NS*R + j%NS + r*NS with j = b >> 3; mode
-    // q = i*R + r of this thread owns tensor-memory columns [4q, 4q + 4) of every block.
+    // s = b % TW (b = tid + i*NT), z index (j/NS)*NS*R + j%NS + r*NS with j = b / TW; mode
+    // q = i*R + r of this thread owns tensor-memory columns [WPC*q, WPC*(q + 1)) of every block.
     const int iy = signed_mode(my, N);
     const int p = f >> 1;
     const int ca = (p >= 3) + (p >= 5), cbp = p < 3 ? p : (p < 5 ? p - 2 : 2);
-    auto sink = [&](int i, double2* v) {
+    auto sink = [&](int i, C* v) {
       constexpr int R = RO::R, NS = RO::NS;
-      const int bb = tid + i * NT, s_ = bb & 7, j = bb >> 3;
-      const uint32_t col = (uint32_t)(4 * R * i);
+      const int bb = tid + i * NT, s_ = bb % TW, j = bb / TW;
+      const uint32_t col = (uint32_t)(WPC * R * i);
       if ((f & 1) == 0) {
         tmem_st<R>(tq + col, v);  // park P0 of this pair
         return;
@@ -1031,7 +1076,7 @@ k_p5(const __grid_constant__ CUtensorMap map, double2* __restrict__ u, double2* 
       const int ix = mx0 + s_;
       int izs[R];
       {
-        double2 p0[R];
+        C p0[R];
         tmem_ld<R>(tq + col, p0);
 #pragma unroll
         for (int r = 0; r < R; ++r) {
@@ -1047,43 +1092,43 @@ k_p5(const __grid_constant__ CUtensorMap map, double2* __restrict__ u, double2* 
         const int dst = side == 0 ? ca : cbp, kc = side == 0 ? cbp : ca;
         const bool first = side == 0 ? (p == 0) : (p == 1 || p == 2);  // r_x at 00, r_y at 01, r_z at 02
         const uint32_t ta = tq + (uint32_t)(CW * (1 + dst)) + col;
-        double2 r[R];
+        C r[R];
         if (!first) tmem_ld<R>(ta, r);
 #pragma unroll
         for (int rr = 0; rr < R; ++rr) {
           const int kk = kc == 0 ? ix : (kc == 1 ? iy : izs[rr]);
-          const double2 c = minus_i_k(v[rr], kk);
+          const C c = minus_i_k(v[rr], kk);
           r[rr] = first ? c : cadd(r[rr], c);
         }
         tmem_st<R>(ta, r);
       }
     };
-    tile_fft_sink<N, -1, NT>([&](int s_, int e_) { return IN[e_ * 8 + s_]; }, W, s_tw, tid, sink);
+    tile_fft_sink<N, -1, NT, TW>([&](int s_, int e_) { return IN[e_ * TW + s_]; }, W, s_tw, tid, sink);
     tmem_wait_st();
     __syncthreads();  // IN[b] and W are free again
     if (tid == 0 && ul + 2 < nunits) issue(ul + 2, b);
-    auto mode_s = [&](int q) { return (tid + (q / RO::R) * NT) & 7; };
+    auto mode_s = [&](int q) { return (tid + (q / RO::R) * NT) % TW; };
     auto mode_e = [&](int q) {
-      const int j = (tid + (q / RO::R) * NT) >> 3, r = q % RO::R;
+      const int j = (tid + (q / RO::R) * NT) / TW, r = q % RO::R;
       return (j / RO::NS) * RO::NS * RO::R + (j % RO::NS) + r * RO::NS;
     };
     if (f == 11) {
 #pragma unroll 1
       for (int q = 0; q < MPT; ++q) {
-        double2 r3[3];
+        C r3[3];
 #pragma unroll
-        for (int c = 0; c < 3; ++c) r3[c] = tmem_ld1(tq + CW * (1 + c) + 4 * q);
+        for (int c = 0; c < 3; ++c) r3[c] = tmem_ld1<C>(tq + CW * (1 + c) + WPC * q);
         const int ix = mx0 + mode_s(q);
         if (ix >= NH) continue;
         const int ez = mode_e(q);
         const int iz = signed_mode(ez, N);
         const long long row = (long long)ez * N + my;
         const long long idx = row * g.pitch + ix;
-        double2 uu[3], gg[3], rr[3];
+        C uu[3], gg[3], rr[3];
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
           uu[c] = u[(long long)c * g.field + idx];
-          gg[c] = load_g ? gbuf[(long long)c * g.field + idx] : make_double2(0, 0);
+          gg[c] = load_g ? gbuf[(long long)c * g.field + idx] : czero<C>();
         }
         finish_mode(r3, ix, iy, iz, N, uu, gg, load_g, rr, a);
         const bool nyq_zero = ix == 0 && row != 0;  // plane mx = N/2 is zero off (N/2,0,0)
@@ -1092,13 +1137,13 @@ k_p5(const __grid_constant__ CUtensorMap map, double2* __restrict__ u, double2* 
         for (int c = 0; c < 3; ++c) {
           if (a.mode != 0) {
             rhs[(long long)c * g.field + idx] = rr[c];
-            if (nyq_zero) rhs[(long long)c * g.field + inq] = make_double2(0.0, 0.0);
+            if (nyq_zero) rhs[(long long)c * g.field + inq] = czero<C>();
           } else {
             u[(long long)c * g.field + idx] = uu[c];
             gbuf[(long long)c * g.field + idx] = gg[c];
             if (nyq_zero) {
-              u[(long long)c * g.field + inq] = make_double2(0.0, 0.0);
-              gbuf[(long long)c * g.field + inq] = make_double2(0.0, 0.0);
+              u[(long long)c * g.field + inq] = czero<C>();
+              gbuf[(long long)c * g.field + inq] = czero<C>();
             }
           }
         }
@@ -1112,48 +1157,51 @@ k_p5(const __grid_constant__ CUtensorMap map, double2* __restrict__ u, double2* 
 // ------------------------------------------------------------------------------------
 // Generic x transforms (FFT-backend contract and initialisation).  Two rows of one field
 // share a complex FFT.  grid (N*N/2, nf).
-template <int N>
+template <int N, class C>
 __global__ void __launch_bounds__(nt_x<N>())
-k_xpass_r2c(const double* __restrict__ in, double2* __restrict__ out, const double2* __restrict__ tw, Geom g) {
+k_xpass_r2c(const double* __restrict__ in, C* __restrict__ out, const C* __restrict__ tw, Geom g) {
   constexpr int NT = nt_x<N>();
   constexpr int NH = N / 2;
   constexpr int RP = row_pitch(N);
-  extern __shared__ double2 smem[];
-  double2* s_tw = smem;
-  double2* seq = smem + N;
+  extern __shared__ __align__(16) unsigned char smraw_x[];
+  C* smem = reinterpret_cast<C*>(smraw_x);
+  C* s_tw = smem;
+  C* seq = smem + N;
   const int tid = threadIdx.x;
   load_twiddles<N>(s_tw, tw, tid, NT);
   const long long r0 = 2LL * blockIdx.x;
   const double* fin = in + (long long)blockIdx.y * N * N * N;
-  double2* fout = out + (long long)blockIdx.y * g.field;
-  for (int x = tid; x < N; x += NT) seq[x + (x >> 3)] = make_double2(fin[r0 * N + x], fin[(r0 + 1) * N + x]);
+  C* fout = out + (long long)blockIdx.y * g.field;
+  using RT = real_of<C>;
+  for (int x = tid; x < N; x += NT) seq[x + (x >> 3)] = cmk((RT)fin[r0 * N + x], (RT)fin[(r0 + 1) * N + x]);
   __syncthreads();
   smem_fft<N, -1, 1, NT, RowTile<RP>>(seq, s_tw, tid);
   for (int k = tid; k <= NH; k += NT) {
     const int km = (N - k) % N;
-    double2 A, B;
+    C A, B;
     unpack_pair(seq[k + (k >> 3)], seq[km + (km >> 3)], &A, &B);
     fout[r0 * g.pitch + k] = A;
     fout[(r0 + 1) * g.pitch + k] = B;
   }
 }
 
-template <int N>
+template <int N, class C>
 __global__ void __launch_bounds__(nt_x<N>())
-k_xpass_c2r(const double2* __restrict__ in, double* __restrict__ out, const double2* __restrict__ tw, Geom g) {
+k_xpass_c2r(const C* __restrict__ in, double* __restrict__ out, const C* __restrict__ tw, Geom g) {
   constexpr int NT = nt_x<N>();
   constexpr int NH = N / 2;
   constexpr int RP = row_pitch(N);
-  extern __shared__ double2 smem[];
-  double2* s_tw = smem;
-  double2* seq = smem + N;
+  extern __shared__ __align__(16) unsigned char smraw_x[];
+  C* smem = reinterpret_cast<C*>(smraw_x);
+  C* s_tw = smem;
+  C* seq = smem + N;
   const int tid = threadIdx.x;
   load_twiddles<N>(s_tw, tw, tid, NT);
   const long long r0 = 2LL * blockIdx.x;
-  const double2* fin = in + (long long)blockIdx.y * g.field;
+  const C* fin = in + (long long)blockIdx.y * g.field;
   double* fout = out + (long long)blockIdx.y * N * N * N;
   for (int k = tid; k <= NH; k += NT) {
-    double2 zk, zm;
+    C zk, zm;
     pack_pair(fin[r0 * g.pitch + k], fin[(r0 + 1) * g.pitch + k], k, NH, N, &zk, &zm);
     seq[k + (k >> 3)] = zk;
     if (k != 0 && k != NH) seq[(N - k) + ((N - k) >> 3)] = zm;
@@ -1161,7 +1209,7 @@ k_xpass_c2r(const double2* __restrict__ in, double* __restrict__ out, const doub
   __syncthreads();
   smem_fft<N, +1, 1, NT, RowTile<RP>>(seq, s_tw, tid);
   for (int x = tid; x < N; x += NT) {
-    const double2 v = seq[x + (x >> 3)];
+    const C v = seq[x + (x >> 3)];
     fout[r0 * N + x] = v.x;
     fout[(r0 + 1) * N + x] = v.y;
   }
@@ -1169,33 +1217,34 @@ k_xpass_c2r(const double2* __restrict__ in, double* __restrict__ out, const doub
 
 // Energy / vmax partials of the physical velocity (work fields 0,1,2 after the inverse
 // z and y passes of u_hat without phase shift).  One row per CTA.
-template <int N>
+template <int N, class C>
 __global__ void __launch_bounds__(nt_x<N>())
-k_xpass_diag(const double2* __restrict__ work, const double2* __restrict__ unyq, double scale, int nyq_scalar,
-             double* __restrict__ partials, const double2* __restrict__ tw, Geom g) {
+k_xpass_diag(const C* __restrict__ work, const C* __restrict__ unyq, double scale, int nyq_scalar,
+             double* __restrict__ partials, const C* __restrict__ tw, Geom g) {
   constexpr int NT = nt_x<N>();
   constexpr int NH = N / 2;
   constexpr int RP = row_pitch(N);
-  extern __shared__ double2 smem[];
-  double2* s_tw = smem;
-  double2* seq = smem + N;  // 2 sequences: u0 + i u1, u2
+  extern __shared__ __align__(16) unsigned char smraw_x[];
+  C* smem = reinterpret_cast<C*>(smraw_x);
+  C* s_tw = smem;
+  C* seq = smem + N;  // 2 sequences: u0 + i u1, u2
   __shared__ double red[2 * (NT / 32)];
   const int tid = threadIdx.x;
   load_twiddles<N>(s_tw, tw, tid, NT);
   const long long row = blockIdx.x;
   const long long rbase = row * g.pitch;
   for (int k = tid; k <= NH; k += NT) {
-    double2 U[3];
+    C U[3];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       if (k == NH && nyq_scalar) U[c] = cscale(unyq[(long long)c * g.field + NH], scale);
       else U[c] = work[(long long)c * g.field + rbase + k];
     }
-    double2 zk, zm;
+    C zk, zm;
     pack_pair(U[0], U[1], k, NH, N, &zk, &zm);
     seq[k + (k >> 3)] = zk;
     if (k != 0 && k != NH) seq[(N - k) + ((N - k) >> 3)] = zm;
-    pack_pair(U[2], make_double2(0.0, 0.0), k, NH, N, &zk, &zm);
+    pack_pair(U[2], czero<C>(), k, NH, N, &zk, &zm);
     seq[RP + k + (k >> 3)] = zk;
     if (k != 0 && k != NH) seq[RP + (N - k) + ((N - k) >> 3)] = zm;
   }
@@ -1204,8 +1253,9 @@ k_xpass_diag(const double2* __restrict__ work, const double2* __restrict__ unyq,
   double esum = 0.0, vmax2 = 0.0;
   for (int x = tid; x < N; x += NT) {
     const int p = x + (x >> 3);
-    const double2 a = seq[p], b = seq[RP + p];
-    const double s2 = a.x * a.x + a.y * a.y + b.x * b.x;
+    const C a = seq[p], b = seq[RP + p];
+    const double ax = a.x, ay = a.y, bx = b.x;
+    const double s2 = ax * ax + ay * ay + bx * bx;
     esum += 0.5 * s2;
     vmax2 = fmax(vmax2, s2);
   }
@@ -1235,7 +1285,8 @@ __global__ void k_tgv_init(double* __restrict__ phys, int n) {
 }
 
 // project_truncate over every stored mode, Nyquist column included (:825-844).
-__global__ void k_project_truncate(double2* __restrict__ u, Geom g) {
+template <class C>
+__global__ void k_project_truncate(C* __restrict__ u, Geom g) {
   const long long total = (long long)g.n * g.n * (g.nh + 1);
   const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= total) return;
@@ -1247,31 +1298,37 @@ __global__ void k_project_truncate(double2* __restrict__ u, Geom g) {
   const int m2 = ix * ix + iy * iy + iz * iz;
   const bool keep = 4LL * m2 <= (long long)g.n * g.n;
   const double k2 = (double)m2;
-  double2 ux = u[idx], uy = u[g.field + idx], uz = u[2 * g.field + idx];
+  C ux = u[idx], uy = u[g.field + idx], uz = u[2 * g.field + idx];
   if (k2 > 0.0 && keep) {
-    const double2 dot = cadd(cadd(cscale(ux, (double)ix), cscale(uy, (double)iy)), cscale(uz, (double)iz));
-    const double2 factor = cscale(dot, 1.0 / k2);
+    const C dot = cadd(cadd(cscale(ux, (double)ix), cscale(uy, (double)iy)), cscale(uz, (double)iz));
+    const C factor = cscale(dot, 1.0 / k2);
     ux = csub(ux, cscale(factor, (double)ix));
     uy = csub(uy, cscale(factor, (double)iy));
     uz = csub(uz, cscale(factor, (double)iz));
   } else {
-    ux = uy = uz = make_double2(0.0, 0.0);
+    ux = uy = uz = czero<C>();
   }
   u[idx] = ux;
   u[g.field + idx] = uy;
   u[2 * g.field + idx] = uz;
 }
 
-__global__ void k_add_sparse(double2* __restrict__ u, const long long* __restrict__ idx,
+template <class C>
+__global__ void k_add_sparse(C* __restrict__ u, const long long* __restrict__ idx,
                              const double2* __restrict__ val, int count) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= count) return;
   const long long at = idx[i];
-  u[at] = cadd(u[at], val[i]);
+  using RT = real_of<C>;
+  u[at] = cadd(u[at], cmk((RT)val[i].x, (RT)val[i].y));
 }
 
-// half -> reference full layout (mx < 0 from the conjugate mirror).
-__global__ void k_half_to_full(const double2* __restrict__ half, double2* __restrict__ full, Geom g) {
+// half -> reference full layout (mx < 0 from the conjugate mirror), widened to double.
+__device__ __forceinline__ double2 widen(double2 v) { return v; }
+__device__ __forceinline__ double2 widen(float2 v) { return make_double2(v.x, v.y); }
+
+template <class C>
+__global__ void k_half_to_full(const C* __restrict__ half, double2* __restrict__ full, Geom g) {
   const long long n = g.n;
   const long long total = n * n * n;
   const long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -1279,16 +1336,17 @@ __global__ void k_half_to_full(const double2* __restrict__ half, double2* __rest
   const int x = (int)(id % n);
   const long long y = (id / n) % n, z = id / (n * n);
   if (x <= g.nh) {
-    full[id] = half[(z * n + y) * g.pitch + x];
+    full[id] = widen(half[(z * n + y) * g.pitch + x]);
   } else {
     const long long ym = (n - y) % n, zm = (n - z) % n;
-    full[id] = cconj(half[(zm * n + ym) * g.pitch + (n - x)]);
+    full[id] = widen(cconj(half[(zm * n + ym) * g.pitch + (n - x)]));
   }
 }
 
 // reference full layout -> half; with hermitian_part the Hermitian part
 // (c_m + conj(c_-m))/2 is stored, so a c2r of the result equals Re(IDFT(c)).
-__global__ void k_full_to_half(const double2* __restrict__ full, double2* __restrict__ half, int hermitian_part,
+template <class C>
+__global__ void k_full_to_half(const double2* __restrict__ full, C* __restrict__ half, int hermitian_part,
                                Geom g) {
   const long long n = g.n;
   const long long total = n * n * (g.nh + 1);
@@ -1303,24 +1361,28 @@ __global__ void k_full_to_half(const double2* __restrict__ full, double2* __rest
     const double2 w = full[(zm * n + ym) * n + xm];
     v = make_double2(0.5 * (v.x + w.x), 0.5 * (v.y - w.y));
   }
-  half[row * g.pitch + x] = v;
+  using RT = real_of<C>;
+  half[row * g.pitch + x] = cmk((RT)v.x, (RT)v.y);
 }
 
-// Parseval enstrophy and max spectral divergence of the (masked) state.
+// Parseval enstrophy and max spectral divergence of the (masked) state, in FP64 for
+// either storage precision.
 // Enstrophy = 0.5/N^6 * sum_m |H(omega_hat)_m|^2 over the full spectrum, with
 // omega_hat = i k x u_hat as the reference forms it (:1147-1157).  Planes mx = 0 and
 // mx = N/2 are their own x-mirror: weight 1 and the in-plane Hermitian part; other
 // columns stand for themselves and their conjugate mirror: weight 2.
-__device__ __forceinline__ void omega_hat(const double2* u, long long field, long long idx, int ix, int iy, int iz,
+template <class C>
+__device__ __forceinline__ void omega_hat(const C* u, long long field, long long idx, int ix, int iy, int iz,
                                           double2 w[3]) {
-  const double2 u0 = u[idx], u1 = u[field + idx], u2 = u[2 * field + idx];
+  const double2 u0 = widen(u[idx]), u1 = widen(u[field + idx]), u2 = widen(u[2 * field + idx]);
   const double rx = ix, ry = iy, rz = iz;
   w[0] = make_double2(-(ry * u2.y - rz * u1.y), ry * u2.x - rz * u1.x);
   w[1] = make_double2(-(rz * u0.y - rx * u2.y), rz * u0.x - rx * u2.x);
   w[2] = make_double2(-(rx * u1.y - ry * u0.y), rx * u1.x - ry * u0.x);
 }
 
-__global__ void __launch_bounds__(256) k_spectral_diag(const double2* __restrict__ u, double* __restrict__ partials,
+template <class C>
+__global__ void __launch_bounds__(256) k_spectral_diag(const C* __restrict__ u, double* __restrict__ partials,
                                                        Geom g) {
   __shared__ double red_s[256];
   __shared__ double red_m[256];
@@ -1350,13 +1412,13 @@ __global__ void __launch_bounds__(256) k_spectral_diag(const double2* __restrict
       // mirror -m is not stored; its value is conj(u_m) but its wavenumber keeps +N/2 on the
       // Nyquist axis, so omega_hat(-m) is not conj(omega_hat(m)): form H explicitly.
       const int my2 = yi == g.n / 2 ? iy : -iy, mz2 = zi == g.n / 2 ? iz : -iz;
-      const double2 u0 = u[idx], u1 = u[g.field + idx], u2 = u[2 * g.field + idx];
+      const double2 u0 = widen(u[idx]), u1 = widen(u[g.field + idx]), u2 = widen(u[2 * g.field + idx]);
       const double2 c0 = cconj(u0), c1 = cconj(u1), c2 = cconj(u2);
       const double rx = -ix, ry = my2, rz = mz2;
       double2 wm[3];
-      wm[0] = make_double2(-(ry * c2.y - rz * c1.y), ry * c2.x - rz * c1.x);
-      wm[1] = make_double2(-(rz * c0.y - rx * c2.y), rz * c0.x - rx * c2.x);
-      wm[2] = make_double2(-(rx * c1.y - ry * c0.y), rx * c1.x - ry * c0.x);
+      wm[0] = cmk(-(ry * c2.y - rz * c1.y), ry * c2.x - rz * c1.x);
+      wm[1] = cmk(-(rz * c0.y - rx * c2.y), rz * c0.x - rx * c2.x);
+      wm[2] = cmk(-(rx * c1.y - ry * c0.y), rx * c1.x - ry * c0.x);
       contrib = 0.0;
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
@@ -1371,7 +1433,7 @@ __global__ void __launch_bounds__(256) k_spectral_diag(const double2* __restrict
       for (int c = 0; c < 3; ++c) contrib += 2.0 * (w[c].x * w[c].x + w[c].y * w[c].y);
     }
     s += contrib;
-    const double2 u0 = u[idx], u1 = u[g.field + idx], u2 = u[2 * g.field + idx];
+    const double2 u0 = widen(u[idx]), u1 = widen(u[g.field + idx]), u2 = widen(u[2 * g.field + idx]);
     const double2 div = cadd(cadd(cscale(u0, (double)ix), cscale(u1, (double)iy)), cscale(u2, (double)iz));
     m = fmax(m, sqrt(div.x * div.x + div.y * div.y));
   }
@@ -1417,65 +1479,71 @@ static void set_smem(K kernel, size_t bytes) {
   if (bytes > 48 * 1024) cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
 
-template <int N>
+template <int N, class C>
 struct Launch {
-  static constexpr size_t yz_smem() { return (size_t)(N + kT * N) * sizeof(double2); }
-  static constexpr size_t x_smem(int nseq) { return (size_t)(N + nseq * row_pitch(N)) * sizeof(double2); }
+  static constexpr int kT = tile_cols<C>();
+  static constexpr size_t yz_smem() { return (size_t)(N + kT * N) * sizeof(C); }
+  static constexpr size_t x_smem(int nseq) { return (size_t)(N + nseq * row_pitch(N)) * sizeof(C); }
+  static C* F(void* p) { return static_cast<C*>(p); }
+  static const C* F(const void* p) { return static_cast<const C*>(p); }
 
-  static void zpass_inv_phase(const double2* u, double2* work, const double2* tw, const double2* phase, double scale,
+  static void zpass_inv_phase(const void* u, void* work, const void* tw, const void* phase, double scale,
                               int ntiles, Geom g, cudaStream_t st) {
     dim3 grid(ntiles, N, 3);
-    k_zpass_inv_phase<N><<<grid, nt_yz<N>(), yz_smem(), st>>>(u, work, tw, phase, scale, g);
+    k_zpass_inv_phase<N, C><<<grid, nt_yz<N>(), yz_smem(), st>>>(F(u), F(work), F(tw), F(phase), scale, g);
   }
-  static void ypass(double2* f, int nf, int dir, int ntiles, const double2* tw, Geom g, cudaStream_t st) {
+  static void ypass(void* f, int nf, int dir, int ntiles, const void* tw, Geom g, cudaStream_t st) {
     dim3 grid(ntiles, N, nf);
     if (dir < 0) {
-      k_ypass<N, -1><<<grid, nt_yz<N>(), yz_smem(), st>>>(f, tw, g);
+      k_ypass<N, -1, C><<<grid, nt_yz<N>(), yz_smem(), st>>>(F(f), F(tw), g);
     } else {
-      k_ypass<N, +1><<<grid, nt_yz<N>(), yz_smem(), st>>>(f, tw, g);
+      k_ypass<N, +1, C><<<grid, nt_yz<N>(), yz_smem(), st>>>(F(f), F(tw), g);
     }
   }
-  static void zpass(const double2* src, double2* dst, int nf, int dir, int ntiles, double scale, const double2* tw,
-                    Geom g, cudaStream_t st) {
+  static void zpass(const void* src, void* dst, int nf, int dir, int ntiles, double scale, const void* tw, Geom g,
+                    cudaStream_t st) {
     dim3 grid(ntiles, N, nf);
     if (dir < 0) {
-      k_zpass<N, -1><<<grid, nt_yz<N>(), yz_smem(), st>>>(src, dst, scale, tw, g);
+      k_zpass<N, -1, C><<<grid, nt_yz<N>(), yz_smem(), st>>>(F(src), F(dst), scale, F(tw), g);
     } else {
-      k_zpass<N, +1><<<grid, nt_yz<N>(), yz_smem(), st>>>(src, dst, scale, tw, g);
+      k_zpass<N, +1, C><<<grid, nt_yz<N>(), yz_smem(), st>>>(F(src), F(dst), scale, F(tw), g);
     }
   }
-  static void xpass_products(double2* work, const double2* unyq, const double2* phase, double scale, int nyq_scalar,
-                             double* partials, const double2* tw, Geom g, cudaStream_t st) {
-    k_xpass_products<N><<<N * N, nt_x<N>(), x_smem(6), st>>>(work, unyq, phase, scale, nyq_scalar, partials, tw, g);
+  static void xpass_products(void* work, const void* unyq, const void* phase, double scale, int nyq_scalar,
+                             double* partials, const void* tw, Geom g, cudaStream_t st) {
+    k_xpass_products<N, C><<<N * N, nt_x<N>(), x_smem(6), st>>>(F(work), F(unyq), F(phase), scale, nyq_scalar,
+                                                                  partials, F(tw), g);
   }
-  static void nyq_reduce(const double2* work, double* sums, Geom g, cudaStream_t st) {
-    k_nyq_reduce<<<12, 256, 0, st>>>(work, sums, g);
+  static void nyq_reduce(const void* work, double* sums, Geom g, cudaStream_t st) {
+    k_nyq_reduce<C><<<12, 256, 0, st>>>(F(work), sums, g);
   }
-  static void sweep(const double2* work, double2* u, double2* gbuf, double2* rhs, const double* nyq_part, int nparts,
-                    const double2* phase, SweepArgs a, Geom g, cudaStream_t st) {
+  static void sweep(const void* work, void* u, void* gbuf, void* rhs, const double* nyq_part, int nparts,
+                    const void* phase, SweepArgs a, Geom g, cudaStream_t st) {
     const long long total = (long long)N * N * (N / 2);
-    k_sweep<N><<<(unsigned)((total + 255) / 256), 256, 0, st>>>(work, u, gbuf, rhs, nyq_part, nparts, phase, a, g);
+    k_sweep<N, C><<<(unsigned)((total + 255) / 256), 256, 0, st>>>(F(work), F(u), F(gbuf), F(rhs), nyq_part, nparts,
+                                                                   F(phase), a, g);
   }
-  static void xpass2(double2* work, const double2* unyq, const double2* phase, double scale, int nyq_scalar,
-                     double* nyq_part, const double2* tw2, Geom g, int grid, int* err, cudaStream_t st) {
+  static void xpass2(void* work, const void* unyq, const void* phase, double scale, int nyq_scalar, double* nyq_part,
+                     const void* tw2, Geom g, int grid, int* err, cudaStream_t st) {
     if constexpr (N == 256 || N == 512) {
-      k_xpass2<N><<<grid, XP<N>::NT, XP<N>::smem, st>>>(work, unyq, phase, scale, nyq_scalar, nyq_part, tw2, g, err);
+      k_xpass2<N, C><<<grid, XP<N, C>::NT, XP<N, C>::smem, st>>>(F(work), F(unyq), F(phase), scale, nyq_scalar,
+                                                                  nyq_part, F(tw2), g, err);
     }
   }
-  static void p5(const CUtensorMap& map, double2* u, double2* gbuf, double2* rhs, const double* nyq_part, int nparts,
-                 const double2* tw, const double2* phase, SweepArgs a, int ncb, Geom g, int grid, int* err,
+  static void p5(const CUtensorMap& map, void* u, void* gbuf, void* rhs, const double* nyq_part, int nparts,
+                 const void* tw, const void* phase, SweepArgs a, int ncb, Geom g, int grid, int* err,
                  cudaStream_t st) {
     if constexpr (N == 128 || N == 256 || N == 512) {
-      k_nyq_mode<N><<<1, 32, 0, st>>>(u, gbuf, rhs, nyq_part, nparts, phase, a, g);
-      k_p5<N><<<grid, nt_p5<N>(), tma_smem<N>(), st>>>(map, u, gbuf, rhs, nyq_part, nparts, tw, phase, a, ncb, g,
-                                                        err);
+      k_nyq_mode<N, C><<<1, 32, 0, st>>>(F(u), F(gbuf), F(rhs), nyq_part, nparts, F(phase), a, g);
+      k_p5<N, C><<<grid, nt_p5<N>(), tma_smem<N, C>(), st>>>(map, F(u), F(gbuf), F(rhs), nyq_part, nparts, F(tw),
+                                                              F(phase), a, ncb, g, err);
     }
   }
   // Persistent grid of the fused P5 (0: this size runs forward z + sweep as two kernels).
   static int p5_grid(int nsm) {
     if constexpr (N == 128 || N == 256 || N == 512) {
       int nb = 0;
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_p5<N>, nt_p5<N>(), tma_smem<N>());
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_p5<N, C>, nt_p5<N>(), tma_smem<N, C>());
       // tensor memory holds at most 512 columns per SM
       const int cap = 512 / (int)p5_cols<N>();
       nb = nb < 1 ? 1 : (nb > cap ? cap : nb);
@@ -1489,8 +1557,8 @@ struct Launch {
   static int xpass2_grid(int nsm) {
     if constexpr (N == 256 || N == 512) {
       int nb = 0;
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_xpass2<N>, XP<N>::NT, XP<N>::smem);
-      const long long niter = (long long)N * N / XP<N>::ROWS;
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_xpass2<N, C>, XP<N, C>::NT, XP<N, C>::smem);
+      const long long niter = (long long)N * N / XP<N, C>::ROWS;
       long long grid = (long long)nsm * (nb > 0 ? nb : 1);
       return (int)(grid < niter ? grid : niter);
     } else {
@@ -1498,23 +1566,23 @@ struct Launch {
       return 0;
     }
   }
-  static void xpass_r2c(const double* in, double2* out, int nf, const double2* tw, Geom g, cudaStream_t st) {
-    k_xpass_r2c<N><<<dim3(N * N / 2, nf), nt_x<N>(), x_smem(1), st>>>(in, out, tw, g);
+  static void xpass_r2c(const double* in, void* out, int nf, const void* tw, Geom g, cudaStream_t st) {
+    k_xpass_r2c<N, C><<<dim3(N * N / 2, nf), nt_x<N>(), x_smem(1), st>>>(in, F(out), F(tw), g);
   }
-  static void xpass_c2r(const double2* in, double* out, int nf, const double2* tw, Geom g, cudaStream_t st) {
-    k_xpass_c2r<N><<<dim3(N * N / 2, nf), nt_x<N>(), x_smem(1), st>>>(in, out, tw, g);
+  static void xpass_c2r(const void* in, double* out, int nf, const void* tw, Geom g, cudaStream_t st) {
+    k_xpass_c2r<N, C><<<dim3(N * N / 2, nf), nt_x<N>(), x_smem(1), st>>>(F(in), out, F(tw), g);
   }
-  static void xpass_diag(const double2* work, const double2* unyq, double scale, int nyq_scalar, double* partials,
-                         const double2* tw, Geom g, cudaStream_t st) {
-    k_xpass_diag<N><<<N * N, nt_x<N>(), x_smem(2), st>>>(work, unyq, scale, nyq_scalar, partials, tw, g);
+  static void xpass_diag(const void* work, const void* unyq, double scale, int nyq_scalar, double* partials,
+                         const void* tw, Geom g, cudaStream_t st) {
+    k_xpass_diag<N, C><<<N * N, nt_x<N>(), x_smem(2), st>>>(F(work), F(unyq), scale, nyq_scalar, partials, F(tw), g);
   }
   template <int AXIS, int DIR, int VARIANT>
-  static void yz_tma_launch(const CUtensorMap& map, TmaArgs a, const double2* tw, const double2* phase, Geom g,
-                            int grid, cudaStream_t st) {
-    k_yz_tma<N, AXIS, DIR, VARIANT><<<grid, nt_tma<N>(), tma_smem<N>(), st>>>(map, a, tw, phase, g);
+  static void yz_tma_launch(const CUtensorMap& map, TmaArgs a, const void* tw, const void* phase, Geom g, int grid,
+                            cudaStream_t st) {
+    k_yz_tma<N, AXIS, DIR, VARIANT, C><<<grid, nt_tma<N>(), tma_smem<N, C>(), st>>>(map, a, F(tw), F(phase), g);
   }
-  static void yz_tma(const CUtensorMap& map, int axis, int dir, int variant, TmaArgs a, const double2* tw,
-                     const double2* phase, Geom g, int grid, cudaStream_t st) {
+  static void yz_tma(const CUtensorMap& map, int axis, int dir, int variant, TmaArgs a, const void* tw,
+                     const void* phase, Geom g, int grid, cudaStream_t st) {
     if (variant == 1) yz_tma_launch<2, +1, 1>(map, a, tw, phase, g, grid, st);
     else if (axis == 1 && dir < 0) yz_tma_launch<1, -1, 0>(map, a, tw, phase, g, grid, st);
     else if (axis == 1) yz_tma_launch<1, +1, 0>(map, a, tw, phase, g, grid, st);
@@ -1526,83 +1594,104 @@ struct Launch {
     int lo = 1 << 30;
     auto occ = [&](auto kernel) {
       int nb = 0;
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel, nt_tma<N>(), tma_smem<N>());
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel, nt_tma<N>(), tma_smem<N, C>());
       lo = nb < lo ? nb : lo;
     };
-    occ(k_yz_tma<N, 2, +1, 1>);
-    occ(k_yz_tma<N, 1, -1, 0>);
-    occ(k_yz_tma<N, 1, +1, 0>);
-    occ(k_yz_tma<N, 2, -1, 0>);
-    occ(k_yz_tma<N, 2, +1, 0>);
+    occ(k_yz_tma<N, 2, +1, 1, C>);
+    occ(k_yz_tma<N, 1, -1, 0, C>);
+    occ(k_yz_tma<N, 1, +1, 0, C>);
+    occ(k_yz_tma<N, 2, -1, 0, C>);
+    occ(k_yz_tma<N, 2, +1, 0, C>);
     return lo > 0 && lo < (1 << 30) ? lo : 1;
   }
   // Opt every kernel of this size into its dynamic shared memory (once per process).
   static void init() {
-    if constexpr (N == 256 || N == 512) set_smem(k_xpass2<N>, XP<N>::smem);
-    if constexpr (N == 128 || N == 256 || N == 512) set_smem(k_p5<N>, tma_smem<N>());
-    set_smem(k_yz_tma<N, 2, +1, 1>, tma_smem<N>());
-    set_smem(k_yz_tma<N, 1, -1, 0>, tma_smem<N>());
-    set_smem(k_yz_tma<N, 1, +1, 0>, tma_smem<N>());
-    set_smem(k_yz_tma<N, 2, -1, 0>, tma_smem<N>());
-    set_smem(k_yz_tma<N, 2, +1, 0>, tma_smem<N>());
-    set_smem(k_zpass_inv_phase<N>, yz_smem());
-    set_smem(k_ypass<N, -1>, yz_smem());
-    set_smem(k_ypass<N, +1>, yz_smem());
-    set_smem(k_zpass<N, -1>, yz_smem());
-    set_smem(k_zpass<N, +1>, yz_smem());
-    set_smem(k_xpass_products<N>, x_smem(6));
-    set_smem(k_xpass_r2c<N>, x_smem(1));
-    set_smem(k_xpass_c2r<N>, x_smem(1));
-    set_smem(k_xpass_diag<N>, x_smem(2));
+    if constexpr (N == 256 || N == 512) set_smem(k_xpass2<N, C>, XP<N, C>::smem);
+    if constexpr (N == 128 || N == 256 || N == 512) set_smem(k_p5<N, C>, tma_smem<N, C>());
+    set_smem(k_yz_tma<N, 2, +1, 1, C>, tma_smem<N, C>());
+    set_smem(k_yz_tma<N, 1, -1, 0, C>, tma_smem<N, C>());
+    set_smem(k_yz_tma<N, 1, +1, 0, C>, tma_smem<N, C>());
+    set_smem(k_yz_tma<N, 2, -1, 0, C>, tma_smem<N, C>());
+    set_smem(k_yz_tma<N, 2, +1, 0, C>, tma_smem<N, C>());
+    set_smem(k_zpass_inv_phase<N, C>, yz_smem());
+    set_smem(k_ypass<N, -1, C>, yz_smem());
+    set_smem(k_ypass<N, +1, C>, yz_smem());
+    set_smem(k_zpass<N, -1, C>, yz_smem());
+    set_smem(k_zpass<N, +1, C>, yz_smem());
+    set_smem(k_xpass_products<N, C>, x_smem(6));
+    set_smem(k_xpass_r2c<N, C>, x_smem(1));
+    set_smem(k_xpass_c2r<N, C>, x_smem(1));
+    set_smem(k_xpass_diag<N, C>, x_smem(2));
   }
   static const Ops* table() {
-    static const Ops ops = {N, init, zpass_inv_phase, ypass, zpass, xpass_products, nyq_reduce, sweep,
-                            xpass_r2c, xpass_c2r, xpass_diag, yz_tma, tma_blocks_per_sm, xpass2, xpass2_grid,
+    static const Ops ops = {N,  (int)sizeof(C), kT, init, zpass_inv_phase, ypass, zpass, xpass_products, nyq_reduce,
+                            sweep, xpass_r2c, xpass_c2r, xpass_diag, yz_tma, tma_blocks_per_sm, xpass2, xpass2_grid,
                             p5, p5_grid};
     return &ops;
   }
 };
 
-const Ops* ops_for(int n) {
+template <class C>
+const Ops* ops_for_type(int n) {
   switch (n) {
-    case 8: return Launch<8>::table();
-    case 12: return Launch<12>::table();
-    case 16: return Launch<16>::table();
-    case 24: return Launch<24>::table();
-    case 32: return Launch<32>::table();
-    case 48: return Launch<48>::table();
-    case 64: return Launch<64>::table();
-    case 96: return Launch<96>::table();
-    case 128: return Launch<128>::table();
-    case 256: return Launch<256>::table();
-    case 512: return Launch<512>::table();
+    case 8: return Launch<8, C>::table();
+    case 12: return Launch<12, C>::table();
+    case 16: return Launch<16, C>::table();
+    case 24: return Launch<24, C>::table();
+    case 32: return Launch<32, C>::table();
+    case 48: return Launch<48, C>::table();
+    case 64: return Launch<64, C>::table();
+    case 96: return Launch<96, C>::table();
+    case 128: return Launch<128, C>::table();
+    case 256: return Launch<256, C>::table();
+    case 512: return Launch<512, C>::table();
     default: return nullptr;
   }
 }
 
+const Ops* ops_for(int n, int precision) {
+  if (precision == 0) return ops_for_type<double2>(n);
+  if (precision == 1) return ops_for_type<float2>(n);
+  return nullptr;
+}
+
 static unsigned blocks_for(long long total, int bs) { return (unsigned)((total + bs - 1) / bs); }
+
+template <class C>
+static C* FC(void* p) { return static_cast<C*>(p); }
+template <class C>
+static const C* FC(const void* p) { return static_cast<const C*>(p); }
 
 void launch_tgv_init(double* phys, Geom g, cudaStream_t st) {
   const long long np = (long long)g.n * g.n * g.n;
   k_tgv_init<<<blocks_for(np, 256), 256, 0, st>>>(phys, g.n);
 }
-void launch_project_truncate(double2* u, Geom g, cudaStream_t st) {
+void launch_project_truncate(void* u, int precision, Geom g, cudaStream_t st) {
   const long long total = (long long)g.n * g.n * (g.nh + 1);
-  k_project_truncate<<<blocks_for(total, 256), 256, 0, st>>>(u, g);
+  if (precision == 0) k_project_truncate<double2><<<blocks_for(total, 256), 256, 0, st>>>(FC<double2>(u), g);
+  else k_project_truncate<float2><<<blocks_for(total, 256), 256, 0, st>>>(FC<float2>(u), g);
 }
-void launch_add_sparse(double2* u, const long long* idx, const double2* val, int count, cudaStream_t st) {
-  if (count > 0) k_add_sparse<<<blocks_for(count, 256), 256, 0, st>>>(u, idx, val, count);
+void launch_add_sparse(void* u, int precision, const long long* idx, const double2* val, int count,
+                       cudaStream_t st) {
+  if (count <= 0) return;
+  if (precision == 0) k_add_sparse<double2><<<blocks_for(count, 256), 256, 0, st>>>(FC<double2>(u), idx, val, count);
+  else k_add_sparse<float2><<<blocks_for(count, 256), 256, 0, st>>>(FC<float2>(u), idx, val, count);
 }
-void launch_half_to_full(const double2* half, double2* full, Geom g, cudaStream_t st) {
+void launch_half_to_full(const void* half, int precision, double2* full, Geom g, cudaStream_t st) {
   const long long total = (long long)g.n * g.n * g.n;
-  k_half_to_full<<<blocks_for(total, 256), 256, 0, st>>>(half, full, g);
+  if (precision == 0) k_half_to_full<double2><<<blocks_for(total, 256), 256, 0, st>>>(FC<double2>(half), full, g);
+  else k_half_to_full<float2><<<blocks_for(total, 256), 256, 0, st>>>(FC<float2>(half), full, g);
 }
-void launch_full_to_half(const double2* full, double2* half, int hermitian_part, Geom g, cudaStream_t st) {
+void launch_full_to_half(const double2* full, void* half, int precision, int hermitian_part, Geom g,
+                         cudaStream_t st) {
   const long long total = (long long)g.n * g.n * (g.nh + 1);
-  k_full_to_half<<<blocks_for(total, 256), 256, 0, st>>>(full, half, hermitian_part, g);
+  if (precision == 0)
+    k_full_to_half<double2><<<blocks_for(total, 256), 256, 0, st>>>(full, FC<double2>(half), hermitian_part, g);
+  else k_full_to_half<float2><<<blocks_for(total, 256), 256, 0, st>>>(full, FC<float2>(half), hermitian_part, g);
 }
-void launch_spectral_diag(const double2* u, double* partials, int nblocks, Geom g, cudaStream_t st) {
-  k_spectral_diag<<<nblocks, 256, 0, st>>>(u, partials, g);
+void launch_spectral_diag(const void* u, int precision, double* partials, int nblocks, Geom g, cudaStream_t st) {
+  if (precision == 0) k_spectral_diag<double2><<<nblocks, 256, 0, st>>>(FC<double2>(u), partials, g);
+  else k_spectral_diag<float2><<<nblocks, 256, 0, st>>>(FC<float2>(u), partials, g);
 }
 void launch_reduce(const double* partials, int count, int stride, int op_max, double* out, cudaStream_t st) {
   k_reduce<<<1, 256, 0, st>>>(partials, count, stride, op_max, out);

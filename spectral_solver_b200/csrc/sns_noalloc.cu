@@ -194,7 +194,7 @@ extern "C" int sns_forward_r2c_noalloc(int n, const double* dev_physical, double
   ops->xpass_r2c(dev_physical, work, 1, tw, g, st);
   ops->ypass(work, 1, -1, tiles, tw, g, st);
   ops->zpass(work, work, 1, -1, tiles, 1.0, tw, g, st);
-  sns::launch_half_to_full(work, reinterpret_cast<double2*>(dev_spectral), g, st);
+  sns::launch_half_to_full(work, SNS_PRECISION_FP64, reinterpret_cast<double2*>(dev_spectral), g, st);
   e = cudaGetLastError();
   if (e != cudaSuccess) return fail_cuda("sns_forward_r2c_noalloc: launch", e);
   e = cudaStreamSynchronize(st);

@@ -90,104 +90,136 @@ __device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 __device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
 
-// 8 complex doubles (32 words) of this thread's lane, columns [col, col + 32).
-__device__ __forceinline__ void tmem_st8(uint32_t taddr, const double2* v) {
-  uint32_t w[32];
-#pragma unroll
-  for (int i = 0; i < 8; ++i) {
-    const unsigned long long a = __double_as_longlong(v[i].x), b = __double_as_longlong(v[i].y);
-    w[4 * i + 0] = (uint32_t)a;
-    w[4 * i + 1] = (uint32_t)(a >> 32);
-    w[4 * i + 2] = (uint32_t)b;
-    w[4 * i + 3] = (uint32_t)(b >> 32);
-  }
-  asm volatile(
-      "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
-      "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31, %32};" ::"r"(taddr),
-      "r"(w[0]), "r"(w[1]), "r"(w[2]), "r"(w[3]), "r"(w[4]), "r"(w[5]), "r"(w[6]), "r"(w[7]), "r"(w[8]), "r"(w[9]),
-      "r"(w[10]), "r"(w[11]), "r"(w[12]), "r"(w[13]), "r"(w[14]), "r"(w[15]), "r"(w[16]), "r"(w[17]), "r"(w[18]),
-      "r"(w[19]), "r"(w[20]), "r"(w[21]), "r"(w[22]), "r"(w[23]), "r"(w[24]), "r"(w[25]), "r"(w[26]), "r"(w[27]),
-      "r"(w[28]), "r"(w[29]), "r"(w[30]), "r"(w[31])
-      : "memory");
-}
+// Words of this thread's lane: NW 32-bit words at columns [col, col + NW) (32x32b shape).
+#define SNS_R2(i) "r"(w[i]), "r"(w[i + 1])
+#define SNS_R4(i) SNS_R2(i), SNS_R2(i + 2)
+#define SNS_R8(i) SNS_R4(i), SNS_R4(i + 4)
+#define SNS_R16(i) SNS_R8(i), SNS_R8(i + 8)
+#define SNS_R32(i) SNS_R16(i), SNS_R16(i + 16)
+#define SNS_W2(i) "=r"(w[i]), "=r"(w[i + 1])
+#define SNS_W4(i) SNS_W2(i), SNS_W2(i + 2)
+#define SNS_W8(i) SNS_W4(i), SNS_W4(i + 4)
+#define SNS_W16(i) SNS_W8(i), SNS_W8(i + 8)
+#define SNS_W32(i) SNS_W16(i), SNS_W16(i + 16)
 
-__device__ __forceinline__ void tmem_ld8(uint32_t taddr, double2* v) {
-  uint32_t w[32];
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
-      "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
-      : "=r"(w[0]), "=r"(w[1]), "=r"(w[2]), "=r"(w[3]), "=r"(w[4]), "=r"(w[5]), "=r"(w[6]), "=r"(w[7]), "=r"(w[8]),
-        "=r"(w[9]), "=r"(w[10]), "=r"(w[11]), "=r"(w[12]), "=r"(w[13]), "=r"(w[14]), "=r"(w[15]), "=r"(w[16]),
-        "=r"(w[17]), "=r"(w[18]), "=r"(w[19]), "=r"(w[20]), "=r"(w[21]), "=r"(w[22]), "=r"(w[23]), "=r"(w[24]),
-        "=r"(w[25]), "=r"(w[26]), "=r"(w[27]), "=r"(w[28]), "=r"(w[29]), "=r"(w[30]), "=r"(w[31])
-      : "r"(taddr)
-      : "memory");
-  tmem_wait_ld();
-#pragma unroll
-  for (int i = 0; i < 8; ++i) {
-    v[i].x = __longlong_as_double((long long)(((unsigned long long)w[4 * i + 1] << 32) | w[4 * i + 0]));
-    v[i].y = __longlong_as_double((long long)(((unsigned long long)w[4 * i + 3] << 32) | w[4 * i + 2]));
-  }
-}
-
-// One complex double (4 words) of this thread's lane at columns [col, col + 4).
-__device__ __forceinline__ double2 tmem_ld1(uint32_t taddr) {
-  uint32_t w0, w1, w2, w3;
-  asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0, %1, %2, %3}, [%4];"
-               : "=r"(w0), "=r"(w1), "=r"(w2), "=r"(w3)
-               : "r"(taddr)
-               : "memory");
-  tmem_wait_ld();
-  return make_double2(__longlong_as_double((long long)(((unsigned long long)w1 << 32) | w0)),
-                      __longlong_as_double((long long)(((unsigned long long)w3 << 32) | w2)));
-}
-
-// K complex doubles (4K words, K = 4 or 8) of this thread's lane at columns [col, col + 4K).
-template <int K>
-__device__ __forceinline__ void tmem_st(uint32_t taddr, const double2* v) {
-  if constexpr (K == 8) {
-    tmem_st8(taddr, v);
-  } else {
-    static_assert(K == 4, "4 or 8 complex values");
-    uint32_t w[16];
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      const unsigned long long a = __double_as_longlong(v[i].x), b = __double_as_longlong(v[i].y);
-      w[4 * i + 0] = (uint32_t)a;
-      w[4 * i + 1] = (uint32_t)(a >> 32);
-      w[4 * i + 2] = (uint32_t)b;
-      w[4 * i + 3] = (uint32_t)(b >> 32);
-    }
+template <int NW>
+__device__ __forceinline__ void tmem_st_words(uint32_t taddr, const uint32_t* w) {
+  if constexpr (NW == 2) {
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x2.b32 [%0], {%1, %2};" ::"r"(taddr), SNS_R2(0) : "memory");
+  } else if constexpr (NW == 4) {
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x4.b32 [%0], {%1, %2, %3, %4};" ::"r"(taddr), SNS_R4(0)
+                 : "memory");
+  } else if constexpr (NW == 8) {
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"r"(taddr),
+                 SNS_R8(0)
+                 : "memory");
+  } else if constexpr (NW == 16) {
     asm volatile(
         "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
         "%15, %16};" ::"r"(taddr),
-        "r"(w[0]), "r"(w[1]), "r"(w[2]), "r"(w[3]), "r"(w[4]), "r"(w[5]), "r"(w[6]), "r"(w[7]), "r"(w[8]),
-        "r"(w[9]), "r"(w[10]), "r"(w[11]), "r"(w[12]), "r"(w[13]), "r"(w[14]), "r"(w[15])
+        SNS_R16(0)
+        : "memory");
+  } else {
+    static_assert(NW == 32, "2, 4, 8, 16 or 32 words");
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31, %32};" ::"r"(taddr),
+        SNS_R32(0)
         : "memory");
   }
 }
 
-template <int K>
-__device__ __forceinline__ void tmem_ld(uint32_t taddr, double2* v) {
-  if constexpr (K == 8) {
-    tmem_ld8(taddr, v);
-  } else {
-    static_assert(K == 4, "4 or 8 complex values");
-    uint32_t w[16];
+template <int NW>
+__device__ __forceinline__ void tmem_ld_words(uint32_t taddr, uint32_t* w) {
+  if constexpr (NW == 2) {
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x2.b32 {%0, %1}, [%2];" : SNS_W2(0) : "r"(taddr) : "memory");
+  } else if constexpr (NW == 4) {
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0, %1, %2, %3}, [%4];" : SNS_W4(0) : "r"(taddr)
+                 : "memory");
+  } else if constexpr (NW == 8) {
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                 : SNS_W8(0)
+                 : "r"(taddr)
+                 : "memory");
+  } else if constexpr (NW == 16) {
     asm volatile(
         "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
         "%15}, [%16];"
-        : "=r"(w[0]), "=r"(w[1]), "=r"(w[2]), "=r"(w[3]), "=r"(w[4]), "=r"(w[5]), "=r"(w[6]), "=r"(w[7]),
-          "=r"(w[8]), "=r"(w[9]), "=r"(w[10]), "=r"(w[11]), "=r"(w[12]), "=r"(w[13]), "=r"(w[14]), "=r"(w[15])
+        : SNS_W16(0)
         : "r"(taddr)
         : "memory");
-    tmem_wait_ld();
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      v[i].x = __longlong_as_double((long long)(((unsigned long long)w[4 * i + 1] << 32) | w[4 * i + 0]));
-      v[i].y = __longlong_as_double((long long)(((unsigned long long)w[4 * i + 3] << 32) | w[4 * i + 2]));
-    }
+  } else {
+    static_assert(NW == 32, "2, 4, 8, 16 or 32 words");
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+        : SNS_W32(0)
+        : "r"(taddr)
+        : "memory");
   }
+  tmem_wait_ld();
+}
+
+#undef SNS_R2
+#undef SNS_R4
+#undef SNS_R8
+#undef SNS_R16
+#undef SNS_R32
+#undef SNS_W2
+#undef SNS_W4
+#undef SNS_W8
+#undef SNS_W16
+#undef SNS_W32
+
+// Complex values <-> 32-bit words (4 per complex double, 2 per complex float).
+template <class C>
+constexpr int tmem_words() { return (int)(sizeof(C) / 4); }
+
+__device__ __forceinline__ void to_words(double2 v, uint32_t* w) {
+  const unsigned long long a = __double_as_longlong(v.x), b = __double_as_longlong(v.y);
+  w[0] = (uint32_t)a;
+  w[1] = (uint32_t)(a >> 32);
+  w[2] = (uint32_t)b;
+  w[3] = (uint32_t)(b >> 32);
+}
+__device__ __forceinline__ void to_words(float2 v, uint32_t* w) {
+  w[0] = __float_as_uint(v.x);
+  w[1] = __float_as_uint(v.y);
+}
+__device__ __forceinline__ void from_words(const uint32_t* w, double2* v) {
+  v->x = __longlong_as_double((long long)(((unsigned long long)w[1] << 32) | w[0]));
+  v->y = __longlong_as_double((long long)(((unsigned long long)w[3] << 32) | w[2]));
+}
+__device__ __forceinline__ void from_words(const uint32_t* w, float2* v) {
+  v->x = __uint_as_float(w[0]);
+  v->y = __uint_as_float(w[1]);
+}
+
+// K complex values of this thread's lane at columns [col, col + K * words).
+template <int K, class C>
+__device__ __forceinline__ void tmem_st(uint32_t taddr, const C* v) {
+  constexpr int WPC = tmem_words<C>();
+  uint32_t w[K * WPC];
+#pragma unroll
+  for (int i = 0; i < K; ++i) to_words(v[i], w + WPC * i);
+  tmem_st_words<K * WPC>(taddr, w);
+}
+
+template <int K, class C>
+__device__ __forceinline__ void tmem_ld(uint32_t taddr, C* v) {
+  constexpr int WPC = tmem_words<C>();
+  uint32_t w[K * WPC];
+  tmem_ld_words<K * WPC>(taddr, w);
+#pragma unroll
+  for (int i = 0; i < K; ++i) from_words(w + WPC * i, v + i);
+}
+
+// One complex value of this thread's lane at columns [col, col + words).
+template <class C>
+__device__ __forceinline__ C tmem_ld1(uint32_t taddr) {
+  C v;
+  tmem_ld<1>(taddr, &v);
+  return v;
 }
 
 }  // namespace sns

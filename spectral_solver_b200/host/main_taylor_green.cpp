@@ -1,11 +1,12 @@
 // Command-line driver: the reference's flags (src/main_ava.cpp:43-73) plus
-// --seed --pert-amp --pert-kmax --dump-final.
+// --seed --pert-amp --pert-kmax --dump-final --precision fp64|fp32 --viscous explicit|if.
 #include "spectral/ava_taylor_green.hpp"
 
 #include <algorithm>
 #include <cstdint>
 #include <exception>
 #include <iostream>
+#include <stdexcept>
 #include <string>
 
 namespace {
@@ -49,6 +50,12 @@ int main(int argc, char** argv) {
     c.pert_amp = double_arg(argc, argv, "--pert-amp", c.pert_amp);
     c.pert_kmax = int_arg(argc, argv, "--pert-kmax", c.pert_kmax);
     c.dump_final = int_arg(argc, argv, "--dump-final", 0) != 0;
+    const std::string prec = string_arg(argc, argv, "--precision", "fp64");
+    if (prec != "fp64" && prec != "fp32") throw std::runtime_error("--precision must be fp64 or fp32");
+    c.precision = prec == "fp32" ? 1 : 0;
+    const std::string visc = string_arg(argc, argv, "--viscous", "explicit");
+    if (visc != "explicit" && visc != "if") throw std::runtime_error("--viscous must be explicit or if");
+    c.viscous_mode = visc == "if" ? 1 : 0;
     spectral::ava_solver::run_taylor_green(c);
   } catch (const std::exception& e) {
     std::cerr << "error: " << e.what() << "\n";

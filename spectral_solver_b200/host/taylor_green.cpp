@@ -36,10 +36,11 @@ struct TaylorGreenSolver::Impl {
   double step_time = 0.0, diagnostics_time = 0.0, max_velocity_time = 0.0;
   long long step_calls = 0, diagnostics_calls = 0, max_velocity_calls = 0;
 
-  Impl(int n_in, double reynolds, std::uint64_t seed, double amp, int kmax) : n(n_in) {
+  Impl(int n_in, double reynolds, std::uint64_t seed, double amp, int kmax, int precision, int viscous_mode)
+      : n(n_in) {
     if (n <= 0) throw std::runtime_error("grid size must be positive");
     if (reynolds <= 0.0) throw std::runtime_error("Reynolds number must be positive");
-    const int rc = sns_create(n, 1.0 / reynolds, SNS_PRECISION_FP64, SNS_VISCOUS_EXPLICIT, seed, amp, kmax, &h);
+    const int rc = sns_create(n, 1.0 / reynolds, precision, viscous_mode, seed, amp, kmax, &h);
     if (rc != SNS_OK) throw std::runtime_error(std::string("TaylorGreenSolver: ") + sns_last_error(nullptr));
   }
   ~Impl() {
@@ -50,10 +51,12 @@ struct TaylorGreenSolver::Impl {
   }
 };
 
-TaylorGreenSolver::TaylorGreenSolver(int n, double reynolds) : impl_(std::make_unique<Impl>(n, reynolds, 0, 0.0, 0)) {}
+TaylorGreenSolver::TaylorGreenSolver(int n, double reynolds)
+    : impl_(std::make_unique<Impl>(n, reynolds, 0, 0.0, 0, SNS_PRECISION_FP64, SNS_VISCOUS_EXPLICIT)) {}
 
-TaylorGreenSolver::TaylorGreenSolver(int n, double reynolds, std::uint64_t seed, double pert_amp, int pert_kmax)
-    : impl_(std::make_unique<Impl>(n, reynolds, seed, pert_amp, pert_kmax)) {}
+TaylorGreenSolver::TaylorGreenSolver(int n, double reynolds, std::uint64_t seed, double pert_amp, int pert_kmax,
+                                     int precision, int viscous_mode)
+    : impl_(std::make_unique<Impl>(n, reynolds, seed, pert_amp, pert_kmax, precision, viscous_mode)) {}
 
 TaylorGreenSolver::~TaylorGreenSolver() = default;
 
@@ -127,7 +130,8 @@ void run_taylor_green(const RunConfig& config) {
   csv << "t,kinetic_energy,dissipation,enstrophy,max_spectral_divergence,max_velocity,dt,cfl,main_dt,main_cfl\n";
 
   const double init_t0 = wall();
-  TaylorGreenSolver solver(config.n, config.reynolds, config.seed, config.pert_amp, config.pert_kmax);
+  TaylorGreenSolver solver(config.n, config.reynolds, config.seed, config.pert_amp, config.pert_kmax, config.precision,
+                           config.viscous_mode);
   const double init_time = wall() - init_t0;
   const double run_t0 = wall();
   const double dx = 2.0 * kPi / static_cast<double>(config.n);

@@ -32,6 +32,8 @@ def test_version_and_sizes(lib):
     assert b"sm_100a" in lib.sns_version()
     b512 = lib.sns_bytes_required(512, 0)
     assert 18e9 < b512 < 22e9  # 18 half-spectrum fields at 512^3
+    b512f = lib.sns_bytes_required(512, 1)
+    assert 9.5e9 < b512f < 11e9  # the same 18 fields in FP32 (rows padded to 16 complex floats)
     assert lib.sns_bytes_required(0, 0) == 0
     assert lib.sns_bytes_required(64, 7) == 0
 
@@ -39,8 +41,8 @@ def test_version_and_sizes(lib):
 @pytest.mark.parametrize("args,code", [
     ((0, 1e-3, 0, 0, 0, 0.0, 0), 1),     # n <= 0
     ((64, -1.0, 0, 0, 0, 0.0, 0), 1),    # negative viscosity (Re <= 0)
-    ((64, 1e-3, 1, 0, 0, 0.0, 0), 2),    # precision form not built
-    ((64, 1e-3, 0, 1, 0, 0.0, 0), 2),    # integrating factor not built
+    ((64, 1e-3, 7, 0, 0, 0.0, 0), 2),    # unknown precision
+    ((64, 1e-3, 0, 5, 0, 0.0, 0), 2),    # unknown viscous mode
     ((10, 1e-3, 0, 0, 0, 0.0, 0), 2),    # no FFT plan for 10
     ((64, 1e-3, 0, 0, 0, 1e-3, 32), 1),  # perturbation kmax >= N/2
 ])
