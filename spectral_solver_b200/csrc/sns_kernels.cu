@@ -1113,8 +1113,27 @@ k_p5(const __grid_constant__ CUtensorMap map, C* __restrict__ u, C* __restrict__
       return (j / RO::NS) * RO::NS * RO::R + (j % RO::NS) + r * RO::NS;
     };
     if (f == 11) {
+      // Two-deep software pipeline over this thread's modes: the u, g loads of mode q + 1
+      // are in flight while mode q is combined and stored (different modes, no aliasing).
+      C uu_n[3], gg_n[3];
+      auto load_mode = [&](int q, C* uu, C* gg) {
+        const long long idx = ((long long)mode_e(q) * N + my) * g.pitch + mx0 + mode_s(q);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          uu[c] = u[(long long)c * g.field + idx];
+          gg[c] = load_g ? gbuf[(long long)c * g.field + idx] : czero<C>();
+        }
+      };
+      load_mode(0, uu_n, gg_n);
 #pragma unroll 1
       for (int q = 0; q < MPT; ++q) {
+        C uu[3], gg[3], rr[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          uu[c] = uu_n[c];
+          gg[c] = gg_n[c];
+        }
+        if (q + 1 < MPT) load_mode(q + 1, uu_n, gg_n);
         C r3[3];
 #pragma unroll
         for (int c = 0; c < 3; ++c) r3[c] = tmem_ld1<C>(tq + CW * (1 + c) + WPC * q);
@@ -1124,12 +1143,6 @@ k_p5(const __grid_constant__ CUtensorMap map, C* __restrict__ u, C* __restrict__
         const int iz = signed_mode(ez, N);
         const long long row = (long long)ez * N + my;
         const long long idx = row * g.pitch + ix;
-        C uu[3], gg[3], rr[3];
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-          uu[c] = u[(long long)c * g.field + idx];
-          gg[c] = load_g ? gbuf[(long long)c * g.field + idx] : czero<C>();
-        }
         finish_mode(r3, ix, iy, iz, N, uu, gg, load_g, rr, a);
         const bool nyq_zero = ix == 0 && row != 0;  // plane mx = N/2 is zero off (N/2,0,0)
         const long long inq = row * g.pitch + NH;
