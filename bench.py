@@ -334,8 +334,25 @@ def run_b200(args, world, rank, local, pg):
                 "rel_enstrophy": abs(d32["enstrophy"] - d64["enstrophy"]) / d64["enstrophy"]}
         if cpu is not None:
             line["cpu_baseline"] = cpu
+        extra = run_multi(args) if world == 1 else {}
+        line.update(extra)
         print(json.dumps(line), flush=True)
     return 0
+
+
+def run_multi(args):
+    """The batched-ensemble and serving legs of the metric, shortened so the run stays within
+    minutes: the 64-solve ensemble for --ensemble-steps graph steps per form, and the
+    serving stream's first --serve-seconds of arrivals served to completion per form."""
+    out = {}
+    if args.ensemble_steps > 0:
+        from spectral_solver_b200 import ensemble
+        out["ensemble"] = [ensemble.run(64, args.ensemble_steps, 3, p, 2, None) for p in (1, 0)]
+    if args.serve_seconds > 0:
+        from spectral_solver_b200 import serve
+        stream = serve.make_stream(args.serve_seconds, 20.0)
+        out["serving"] = [serve.run(stream, int(80e9), p) for p in (1, 0)]
+    return out
 
 
 def main():
@@ -346,6 +363,10 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--n", type=int, default=512)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ensemble-steps", type=int, default=50,
+                    help="steps of the 64-solve batched ensemble per form (0: skip)")
+    ap.add_argument("--serve-seconds", type=float, default=2.0,
+                    help="seconds of the serving stream's arrivals served per form (0: skip)")
     ap.add_argument("--precision", default="both", choices=["both", "fp32", "fp64"],
                     help="both: the FP32 precision form is the headline, the FP64 plain form runs beside it")
     args = ap.parse_args()

@@ -137,6 +137,96 @@ int sns_time_steps(sns_handle* h, double dt, int nsteps, double* elapsed_ms);
 #define SNS_NUM_PASSES 7
 int sns_profile_passes(sns_handle* h, double dt, int nsteps, double* pass_ms);
 
+/* ---------------------------------------------------------------------------------------
+ * Batched ensembles (no counterpart in the reference, which runs one solve per process).
+ * Many independent solves of uneven N, Re and precision live on one device; every solve
+ * keeps its own handle (fields resident in HBM) and its own fixed time step.  One RK3 step
+ * of the whole batch is one CUDA graph launch: the graph forks into one branch per solve
+ * (the solve's passes in order on its own stream), so the solves' kernels overlap on the
+ * device.  Results are bitwise those of the same solve stepped alone (fixed-order
+ * reductions, no shared state between solves). */
+typedef struct sns_batch sns_batch;
+
+typedef struct sns_solve_spec {
+  int n;             /* grid size (a supported N) */
+  double nu;         /* viscosity 1/Re */
+  int precision;     /* SNS_PRECISION_* */
+  int viscous_mode;  /* SNS_VISCOUS_* */
+  uint64_t seed;     /* perturbation seed */
+  double pert_amp;   /* perturbation rms amplitude (0: pure Taylor-Green) */
+  int pert_kmax;     /* perturbation shell 1 <= |m| <= pert_kmax */
+  double dt;         /* > 0: fixed time step; <= 0: CFL-limited from the initial field */
+  double cfl;        /* CFL number for dt <= 0 (dt = min(dt_max, cfl * (2 pi / N) / vmax)) */
+  double dt_max;     /* cap of the CFL step */
+} sns_solve_spec;
+
+/* Create `count` solves and capture the batch step graph.  With autotune_trials > 0 the
+ * launch shape of each distinct (N, precision) is chosen by sns_autotune on a scratch handle
+ * (cached in autotune_cache when non-NULL) and used by every solve of that key.  out_dt
+ * (may be NULL) receives each solve's time step. */
+int sns_batch_create(const sns_solve_spec* specs, int count, int autotune_trials, const char* autotune_cache,
+                     sns_batch** out, double* out_dt);
+int sns_batch_destroy(sns_batch* b);
+/* nsteps graph launches (every solve advances nsteps steps), then a synchronisation. */
+int sns_batch_step(sns_batch* b, int nsteps);
+/* Same, timed with CUDA events around the launches; writes the elapsed milliseconds. */
+int sns_batch_time_steps(sns_batch* b, int nsteps, double* elapsed_ms);
+/* The handle of solve i (owned by the batch: get_state, diagnostics, ... work on it). */
+sns_handle* sns_batch_handle(sns_batch* b, int i);
+int sns_batch_size(const sns_batch* b);
+/* Message of the last failed batch call. */
+const char* sns_batch_last_error(const sns_batch* b);
+
+/* Launch-shape autotuner (no counterpart in the reference).  Times the pass variants a
+ * handle can run -- the x pass as the two-stage 16 x M plan or the generic Stockham plan
+ * (N = 256, 512), the forward z pass fused with the k-space sweep or as two kernels
+ * (N >= 128), and the persistent grid of the TMA y/z passes (1 .. max CTAs per SM) -- over
+ * `trial_steps` steps each (the state advances; results do not depend on the choice) and
+ * keeps the fastest.  With a non-NULL cache_path the choice is read from / appended to that
+ * file, one line per (device, N, precision) key, so later handles skip the trials.
+ * out_config (may be NULL) receives {tma_grid, x2_grid, p5_grid}. */
+int sns_autotune(sns_handle* h, int trial_steps, const char* cache_path, int* out_config);
+
+/* ---------------------------------------------------------------------------------------
+ * Serving with continuous batching (no counterpart in the reference).  Requests queue on
+ * the host; each sns_server_step (one tick) admits queued requests in arrival order while
+ * their device bytes fit the HBM budget, advances every resident solve on its own stream
+ * (so their work overlaps on the device) -- the largest resident solve by one step, smaller
+ * ones by N_max^3/N^3 steps (at most 64) -- and retires the solves that reached their
+ * horizon (final diagnostics returned, memory freed), so requests that arrive while others
+ * run are admitted as memory frees up.  Each solve's step is fixed at admission by the CFL
+ * rule on its initial field; each result is bitwise that of the same request solved alone. */
+typedef struct sns_server sns_server;
+
+typedef struct sns_request {
+  int n;             /* grid size */
+  double nu;         /* viscosity 1/Re */
+  double t_end;      /* horizon */
+  uint64_t seed;     /* perturbation seed */
+  double pert_amp;   /* perturbation rms amplitude */
+  int pert_kmax;     /* perturbation shell */
+  double cfl;        /* CFL number of the fixed step chosen at admission */
+  double dt_max;     /* cap of that step */
+} sns_request;
+
+typedef struct sns_result {
+  int64_t id;        /* id returned by sns_server_submit */
+  int n;
+  int steps;         /* RK3 steps taken (the last one clipped to t_end) */
+  double dt;         /* the solve's step */
+  sns_diag final;    /* diagnostics at t_end */
+} sns_result;
+
+int sns_server_create(size_t hbm_budget_bytes, int precision, sns_server** out);
+int sns_server_destroy(sns_server* s);
+int sns_server_submit(sns_server* s, const sns_request* r, int64_t* out_id);
+/* One serving step; finished solves are written to done[0 .. *ndone) (at most max_done,
+ * the rest are returned by later calls).  resident / queued (may be NULL) receive the
+ * counts after the step; bytes_in_use (may be NULL) the admitted device bytes. */
+int sns_server_step(sns_server* s, sns_result* done, int max_done, int* ndone, int* resident, int* queued,
+                    size_t* bytes_in_use);
+const char* sns_server_last_error(const sns_server* s);
+
 /* Forward transform that allocates no device memory (no counterpart in the reference).
  * For callers that cannot let a library call cudaMalloc: applications that reserve the
  * GPU's memory up front and serve it from their own pool, runs close to the HBM limit,

@@ -3,7 +3,7 @@
 // the same records, constructor, methods, run options, CSV columns and stdout lines.
 // RunConfig gains optional fields for the seeded perturbation, the final-field dump, the
 // storage precision and the viscous treatment; their defaults reproduce the reference's run
-// (the reference picks its precision at build time through SPECTRAL_PRECISION).
+// (the reference picks its precision at build time: SPECTRAL_PRECISION, CMakeLists.txt:19-28).
 #pragma once
 
 #include <cstdint>
@@ -47,6 +47,11 @@ struct RunConfig {
   bool dump_final = false;
   int precision = 0;     // 0: FP64 plain form (the drop-in), 1: FP32 precision form
   int viscous_mode = 0;  // 0: explicit viscous term (the reference), 1: integrating factor
+  // checkpoint / resume: every checkpoint_every steps (0: never) the spectral state is
+  // written to <output_dir>/checkpoint.bin; a run with restart = <path> continues from it
+  // (same grid, same CSV columns; rows are appended from the checkpoint's time on)
+  int checkpoint_every = 0;
+  std::string restart;
 };
 
 class TaylorGreenSolver {
@@ -67,6 +72,11 @@ class TaylorGreenSolver {
   void print_profile(int rank, double init_time, double run_time) const;
   // Final physical velocity written as a raw file (header: magic, n, then 3 x n^3 doubles).
   void dump_velocity(const std::string& path);
+  // Exact checkpoint of the spectral state: header "SNSCKPT1", int64 n, int64 precision,
+  // double t, int64 step, then u, v, w as n*n*(n/2+1) complex doubles (modes mx in
+  // [0, n/2], x fastest).  load_checkpoint restores the state and returns t and step.
+  void save_checkpoint(const std::string& path, double t, long long step);
+  void load_checkpoint(const std::string& path, double* t, long long* step);
   sns_handle* handle() const;
 
  private:

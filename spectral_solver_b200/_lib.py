@@ -39,6 +39,21 @@ class SnsDiag(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class SolveSpec(C.Structure):
+    _fields_ = [("n", C.c_int), ("nu", C.c_double), ("precision", C.c_int), ("viscous_mode", C.c_int),
+                ("seed", C.c_uint64), ("pert_amp", C.c_double), ("pert_kmax", C.c_int), ("dt", C.c_double),
+                ("cfl", C.c_double), ("dt_max", C.c_double)]
+
+
+class Request(C.Structure):
+    _fields_ = [("n", C.c_int), ("nu", C.c_double), ("t_end", C.c_double), ("seed", C.c_uint64),
+                ("pert_amp", C.c_double), ("pert_kmax", C.c_int), ("cfl", C.c_double), ("dt_max", C.c_double)]
+
+
+class Result(C.Structure):
+    _fields_ = [("id", C.c_int64), ("n", C.c_int), ("steps", C.c_int), ("dt", C.c_double), ("final", SnsDiag)]
+
+
 SIGNATURES = {
     "sns_version": (C.c_char_p, []),
     "sns_bytes_required": (C.c_size_t, [C.c_int, C.c_int]),
@@ -64,6 +79,20 @@ SIGNATURES = {
     "sns_debug_fail_after": (C.c_int, [_H, C.c_int]),
     "sns_profile_passes": (C.c_int, [_H, C.c_double, C.c_int, _DP]),
     "sns_forward_r2c_noalloc": (C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "sns_batch_create": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_char_p, C.POINTER(C.c_void_p), _DP]),
+    "sns_batch_destroy": (C.c_int, [C.c_void_p]),
+    "sns_batch_step": (C.c_int, [C.c_void_p, C.c_int]),
+    "sns_batch_time_steps": (C.c_int, [C.c_void_p, C.c_int, _DP]),
+    "sns_batch_handle": (C.c_void_p, [C.c_void_p, C.c_int]),
+    "sns_batch_size": (C.c_int, [C.c_void_p]),
+    "sns_batch_last_error": (C.c_char_p, [C.c_void_p]),
+    "sns_autotune": (C.c_int, [_H, C.c_int, C.c_char_p, C.POINTER(C.c_int)]),
+    "sns_server_create": (C.c_int, [C.c_size_t, C.c_int, C.POINTER(C.c_void_p)]),
+    "sns_server_destroy": (C.c_int, [C.c_void_p]),
+    "sns_server_submit": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_int64)]),
+    "sns_server_step": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                  C.POINTER(C.c_int), C.POINTER(C.c_size_t)]),
+    "sns_server_last_error": (C.c_char_p, [C.c_void_p]),
 }
 
 PASS_NAMES = ("p1_zinv_phase", "p2_yinv", "p3_xpass", "p3_nyq", "p4_yfwd", "p5_zfwd", "p5_sweep")
@@ -225,3 +254,133 @@ class Solver:
 
     def device_bytes(self) -> int:
         return int(self.lib.sns_device_bytes(self.h))
+
+    def autotune(self, trial_steps: int = 2, cache_path: str | None = None) -> dict:
+        """Pick the fastest launch shape for this handle (the state advances by the trials)."""
+        out = (C.c_int * 3)()
+        self._check(self.lib.sns_autotune(self.h, trial_steps, cache_path.encode() if cache_path else None, out))
+        return dict(tma_grid=out[0], xpass_grid=out[1], p5_grid=out[2])
+
+
+
+class _BorrowedSolver(Solver):
+    """A Solver view of a handle owned by a batch (closing it does nothing)."""
+
+    def __init__(self, lib, h, n, precision):
+        self.lib = lib
+        self.h = C.c_void_p(h)
+        self.n = n
+        self.precision = precision
+
+    def close(self):
+        self.h = None
+
+
+class Batch:
+    """Many independent solves stepped together: one CUDA graph launch per batch step."""
+
+    def __init__(self, specs, autotune_trials: int = 0, autotune_cache: str | None = None):
+        self.lib = load()
+        arr = (SolveSpec * len(specs))()
+        for i, sp in enumerate(specs):
+            arr[i] = SolveSpec(sp["n"], sp["nu"], sp.get("precision", PRECISION_FP64),
+                               sp.get("viscous_mode", VISCOUS_EXPLICIT), sp.get("seed", 0), sp.get("pert_amp", 0.0),
+                               sp.get("pert_kmax", 0), sp.get("dt", 0.0), sp.get("cfl", 0.5), sp.get("dt_max", 0.5))
+        self.specs = list(specs)
+        dts = (C.c_double * len(specs))()
+        b = C.c_void_p()
+        rc = self.lib.sns_batch_create(C.cast(arr, C.c_void_p), len(specs), autotune_trials,
+                                       autotune_cache.encode() if autotune_cache else None, C.byref(b), dts)
+        if rc != SNS_OK:
+            raise SnsError(rc, self.lib.sns_last_error(None).decode())
+        self.b = b
+        self.dt = list(dts)
+
+    def _check(self, rc):
+        if rc != SNS_OK:
+            raise SnsError(rc, self.lib.sns_batch_last_error(self.b).decode())
+
+    def step(self, nsteps: int = 1):
+        self._check(self.lib.sns_batch_step(self.b, nsteps))
+
+    def time_steps(self, nsteps: int) -> float:
+        ms = C.c_double()
+        self._check(self.lib.sns_batch_time_steps(self.b, nsteps, C.byref(ms)))
+        return ms.value
+
+    def solver(self, i: int) -> Solver:
+        h = self.lib.sns_batch_handle(self.b, i)
+        if not h:
+            raise IndexError(i)
+        sp = self.specs[i]
+        return _BorrowedSolver(self.lib, h, sp["n"], sp.get("precision", PRECISION_FP64))
+
+    def __len__(self):
+        return int(self.lib.sns_batch_size(self.b))
+
+    def close(self):
+        if getattr(self, "b", None):
+            self.lib.sns_batch_destroy(self.b)
+            self.b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+
+class Server:
+    """Continuous-batching server: admission by HBM budget, all resident solves stepped together."""
+
+    def __init__(self, hbm_budget_bytes: int, precision: int = PRECISION_FP32):
+        self.lib = load()
+        s = C.c_void_p()
+        rc = self.lib.sns_server_create(int(hbm_budget_bytes), precision, C.byref(s))
+        if rc != SNS_OK:
+            raise SnsError(rc, self.lib.sns_last_error(None).decode())
+        self.s = s
+        self.precision = precision
+
+    def _check(self, rc):
+        if rc != SNS_OK:
+            raise SnsError(rc, self.lib.sns_server_last_error(self.s).decode())
+
+    def submit(self, n, nu, t_end, seed=0, pert_amp=0.0, pert_kmax=0, cfl=0.5, dt_max=0.5) -> int:
+        r = Request(n, nu, t_end, seed, pert_amp, pert_kmax, cfl, dt_max)
+        rid = C.c_int64()
+        self._check(self.lib.sns_server_submit(self.s, C.byref(r), C.byref(rid)))
+        return rid.value
+
+    def step(self, max_done: int = 256):
+        done = (Result * max_done)()
+        nd, res, q = C.c_int(), C.c_int(), C.c_int()
+        used = C.c_size_t()
+        self._check(self.lib.sns_server_step(self.s, C.cast(done, C.c_void_p), max_done, C.byref(nd), C.byref(res),
+                                             C.byref(q), C.byref(used)))
+        out = [dict(id=done[i].id, n=done[i].n, steps=done[i].steps, dt=done[i].dt, final=done[i].final.as_dict())
+               for i in range(nd.value)]
+        return out, res.value, q.value, used.value
+
+    def close(self):
+        if getattr(self, "s", None):
+            self.lib.sns_server_destroy(self.s)
+            self.s = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()

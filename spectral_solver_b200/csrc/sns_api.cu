@@ -17,6 +17,7 @@
 
 #include <cmath>
 #include <cstdint>
+#include <cstdio>
 #include <cstring>
 #include <exception>
 #include <new>
@@ -451,6 +452,42 @@ void release(sns_handle* h) {
 
 }  // namespace
 
+namespace sns {
+
+// Hooks for the batch and serving layers in this library (not part of the C ABI).
+void enqueue_step(sns_handle* h, double dt) { step_once(h, dt); }
+cudaStream_t handle_stream(const sns_handle* h) { return h->stream; }
+int handle_device(const sns_handle* h) { return h->device; }
+// Synchronise the handle's stream and check its device error word; SNS code, message in h.
+int finish_handle(sns_handle* h, const char* what) {
+  try {
+    sync(h, what);
+    return SNS_OK;
+  } catch (const SnsError& e) {
+    h->err = e.msg;
+    return e.code;
+  }
+}
+const char* handle_error(const sns_handle* h) { return h->err.c_str(); }
+// Launch shape {tma_grid, x2_grid, p5_grid} as sns_autotune reports it; false if the handle
+// cannot run it (its Nyquist partial buffer is sized for its own two-stage x-pass grid).
+bool set_launch_shape(sns_handle* h, const int* cfg) {
+  int nsm = 0;
+  if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device) != cudaSuccess) return false;
+  const int x2_full = h->ops->xpass2_grid(nsm), p5_full = h->ops->p5_grid(nsm);
+  const int tma_max = h->ops->tma_blocks_per_sm();
+  if (cfg[0] < nsm || cfg[0] > nsm * tma_max || (cfg[1] != 0 && cfg[1] != x2_full) ||
+      (cfg[2] != 0 && cfg[2] != p5_full))
+    return false;
+  h->tma_grid = cfg[0];
+  h->x2_grid = cfg[1];
+  h->p5_grid = cfg[2];
+  return true;
+}
+void set_handle_error(sns_handle* h, const char* msg) { h->err = msg; }
+
+}  // namespace sns
+
 extern "C" {
 
 const char* sns_version(void) { return "sns_b200 0.2 (sm_100a, fp64 plain form, fp32 precision form)"; }
@@ -634,6 +671,88 @@ int sns_launch_config(const sns_handle* h, int* out, int count) {
 
 int sns_grid_size(const sns_handle* h) { return h ? h->n : 0; }
 size_t sns_device_bytes(const sns_handle* h) { return h ? h->bytes : 0; }
+
+int sns_autotune(sns_handle* h, int trial_steps, const char* cache_path, int* out_config) {
+  return guarded(h, [&] {
+    if (trial_steps <= 0) throw SnsError(SNS_ERR_INVALID, "trial_steps must be positive");
+    cudaDeviceProp prop{};
+    ck(cudaGetDeviceProperties(&prop, h->device), "cudaGetDeviceProperties");
+    std::string dev = prop.name;
+    for (char& c : dev)
+      if (c == ' ' || c == '\t') c = '_';
+    const std::string key = dev + " " + std::to_string(h->n) + " " + std::to_string(h->precision);
+    int nsm = 0;
+    ck(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device), "cudaDeviceGetAttribute");
+    const int x2_full = h->ops->xpass2_grid(nsm), p5_full = h->ops->p5_grid(nsm);
+    const int tma_max = h->ops->tma_blocks_per_sm();
+    auto apply = [&](int tma, int x2, int p5) {
+      // only shapes this handle was built for: its Nyquist partial buffer is sized for x2_full
+      if (tma < nsm || tma > nsm * tma_max || (x2 != 0 && x2 != x2_full) || (p5 != 0 && p5 != p5_full))
+        return false;
+      h->tma_grid = tma;
+      h->x2_grid = x2;
+      h->p5_grid = p5;
+      return true;
+    };
+    bool cached = false;
+    if (cache_path != nullptr) {
+      if (FILE* f = std::fopen(cache_path, "r")) {
+        char line[512];
+        while (std::fgets(line, sizeof line, f)) {
+          char name[256];
+          int n = 0, prec = 0, tma = 0, x2 = 0, p5 = 0;
+          if (std::sscanf(line, "sns-autotune %255s %d %d %d %d %d", name, &n, &prec, &tma, &x2, &p5) == 6 &&
+              dev == name && n == h->n && prec == h->precision)
+            cached = apply(tma, x2, p5);
+        }
+        std::fclose(f);
+      }
+    }
+    if (!cached) {
+      struct Shape {
+        int tma, x2, p5;
+      };
+      std::vector<Shape> shapes;
+      for (int k = 1; k <= tma_max && k <= 4; ++k)
+        for (int x2 : {x2_full, 0})
+          for (int p5 : {p5_full, 0}) {
+            const Shape sh{nsm * k, x2, p5};
+            bool dup = false;
+            for (const Shape& o : shapes) dup = dup || (o.tma == sh.tma && o.x2 == sh.x2 && o.p5 == sh.p5);
+            if (!dup) shapes.push_back(sh);
+          }
+      double best = 1e300;
+      Shape pick = {h->tma_grid, h->x2_grid, h->p5_grid};
+      for (const Shape& sh : shapes) {
+        apply(sh.tma, sh.x2, sh.p5);
+        step_once(h, 1.0e-4);  // warm-up of this shape
+        ck(cudaEventRecord(h->ev0, h->stream), "event");
+        for (int k = 0; k < trial_steps; ++k) step_once(h, 1.0e-4);
+        ck(cudaEventRecord(h->ev1, h->stream), "event");
+        sync(h, "sns_autotune");
+        float ms = 0.f;
+        ck(cudaEventElapsedTime(&ms, h->ev0, h->ev1), "elapsed");
+        if (ms < best) {
+          best = ms;
+          pick = sh;
+        }
+      }
+      apply(pick.tma, pick.x2, pick.p5);
+      if (cache_path != nullptr) {
+        if (FILE* f = std::fopen(cache_path, "a")) {
+          std::fprintf(f, "sns-autotune %s %d %d %d %d %d\n", dev.c_str(), h->n, h->precision, pick.tma, pick.x2,
+                       pick.p5);
+          std::fclose(f);
+        }
+      }
+    }
+    if (out_config) {
+      out_config[0] = h->tma_grid;
+      out_config[1] = h->x2_grid;
+      out_config[2] = h->p5_grid;
+    }
+  });
+}
 
 int sns_debug_fail_after(sns_handle* h, int k) {
   if (h == nullptr) return SNS_ERR_INVALID;

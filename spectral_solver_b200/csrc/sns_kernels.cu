@@ -38,8 +38,10 @@ __device__ __forceinline__ void load_twiddles(C* sm_tw, const C* tw, int tid, in
 
 template <int N>
 constexpr int nt_yz() { return N < 32 ? 32 : (N > 256 ? 256 : N); }
+// x-pass block: N/2 threads clamped to [32, 256] and rounded up to whole warps (the block
+// reductions and their full-mask shuffles need every warp complete: N = 96 gives 64)
 template <int N>
-constexpr int nt_x() { return N / 2 < 32 ? 32 : (N / 2 > 256 ? 256 : N / 2); }
+constexpr int nt_x() { return ((N / 2 < 32 ? 32 : (N / 2 > 256 ? 256 : N / 2)) + 31) / 32 * 32; }
 
 // ------------------------------------------------------------------------------------
 // P1: inverse z transform with the fused phase shift.
@@ -309,6 +311,7 @@ __device__ __forceinline__ void unpack_pair(C Zk, C Zm, C* A, C* B) {
 
 template <int NT>
 __device__ __forceinline__ void block_sum_max(double& s, double& m, double* red) {
+  static_assert(NT % 32 == 0, "whole warps");
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
     s += __shfl_xor_sync(0xffffffffu, s, o);

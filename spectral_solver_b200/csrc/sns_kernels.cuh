@@ -111,6 +111,21 @@ void launch_full_to_half(const double2* full, void* half, int precision, int her
 void launch_spectral_diag(const void* u, int precision, double* partials, int nblocks, Geom g, cudaStream_t st);
 void launch_reduce(const double* partials, int count, int stride, int op_max, double* out, cudaStream_t st);
 
+}  // namespace sns
+
+struct sns_handle;
+
+namespace sns {
+
+// Handle hooks for the batch and serving layers (defined in sns_api.cu).
+void enqueue_step(sns_handle* h, double dt);  // one RK3 step on the handle's stream, no sync
+cudaStream_t handle_stream(const sns_handle* h);
+int handle_device(const sns_handle* h);
+int finish_handle(sns_handle* h, const char* what);  // sync + device error word -> SNS code
+const char* handle_error(const sns_handle* h);
+bool set_launch_shape(sns_handle* h, const int* cfg);  // {tma_grid, x2_grid, p5_grid}
+void set_handle_error(sns_handle* h, const char* msg);
+
 // Host helpers shared by the C-ABI files (sns_api.cu).
 void fill_twiddles(int L, double2* tw);        // exp(-2*pi*i*t/L), t < L
 void set_handleless_error(const char* msg);    // message for sns_last_error(NULL)

@@ -1,0 +1,454 @@
+// Many solves on one device: the batched ensemble (one CUDA graph per batch step, one branch
+// per solve) and the continuous-batching server (HBM-budget admission, per-solve step graphs
+// on per-solve streams, retirement at the horizon).  Neither exists in the reference, which
+// runs one solve per process; both drive the same per-solve handles as sns_step, so every
+// solve computes exactly what it computes alone.
+#include "sns_kernels.cuh"
+#include "../../include/sns_b200.h"
+
+#include <cuda_runtime.h>
+
+#include <array>
+#include <cmath>
+#include <cstdint>
+#include <deque>
+#include <map>
+#include <utility>
+#include <new>
+#include <string>
+#include <vector>
+
+namespace {
+
+constexpr double kPi = 3.141592653589793238462643383279502884;
+
+std::string cuda_msg(const char* what, cudaError_t e) { return std::string(what) + ": " + cudaGetErrorString(e); }
+
+// Fixed step of a solve: the given dt, or the CFL step from the initial field's vmax
+// (the reference's rule, ava_taylor_green_impl.hpp:1363-1368, evaluated once).
+int choose_dt(sns_handle* h, int n, double dt, double cfl, double dt_max, double* out, std::string* err) {
+  if (dt > 0.0) {
+    *out = dt;
+    return SNS_OK;
+  }
+  if (!(cfl > 0.0) || !(dt_max > 0.0)) {
+    *err = "a CFL step needs cfl > 0 and dt_max > 0";
+    return SNS_ERR_INVALID;
+  }
+  double vmax = 0.0;
+  const int rc = sns_max_velocity(h, &vmax);
+  if (rc != SNS_OK) {
+    *err = sns_last_error(h);
+    return rc;
+  }
+  const double dx = 2.0 * kPi / (double)n;
+  double d = dt_max;
+  if (vmax > 1.0e-14) d = std::fmin(d, cfl * dx / vmax);
+  *out = d;
+  return SNS_OK;
+}
+
+// One RK3 step of `h` with step dt captured into an executable graph on the handle's stream.
+int capture_step(sns_handle* h, double dt, cudaGraphExec_t* exec, std::string* err) {
+  cudaStream_t st = sns::handle_stream(h);
+  cudaGraph_t graph = nullptr;
+  cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) {
+    *err = cuda_msg("cudaStreamBeginCapture", e);
+    return SNS_ERR_CUDA;
+  }
+  sns::enqueue_step(h, dt);
+  e = cudaStreamEndCapture(st, &graph);
+  if (e != cudaSuccess) {
+    *err = cuda_msg("cudaStreamEndCapture", e);
+    return SNS_ERR_CUDA;
+  }
+  e = cudaGraphInstantiate(exec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (e != cudaSuccess) {
+    *err = cuda_msg("cudaGraphInstantiate", e);
+    return SNS_ERR_CUDA;
+  }
+  return SNS_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------------------
+// Batched ensemble.
+struct sns_batch {
+  std::vector<sns_handle*> h;
+  std::vector<double> dt;
+  std::vector<cudaEvent_t> join;
+  cudaStream_t origin = nullptr;
+  cudaEvent_t fork = nullptr, ev0 = nullptr, ev1 = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  int device = 0;
+  std::string err;
+};
+
+namespace {
+
+void batch_release(sns_batch* b) {
+  if (!b) return;
+  cudaSetDevice(b->device);
+  if (b->origin) cudaStreamSynchronize(b->origin);
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  for (cudaEvent_t e : b->join)
+    if (e) cudaEventDestroy(e);
+  if (b->fork) cudaEventDestroy(b->fork);
+  if (b->ev0) cudaEventDestroy(b->ev0);
+  if (b->ev1) cudaEventDestroy(b->ev1);
+  if (b->origin) cudaStreamDestroy(b->origin);
+  for (sns_handle* h : b->h)
+    if (h) sns_destroy(h);
+  delete b;
+}
+
+int batch_fail(sns_batch* b, int code, const std::string& msg) {
+  b->err = msg;
+  return code;
+}
+
+// Capture one batch step: fork from the origin stream into every solve's stream, the
+// solve's step there, join back.  The graph's branches are independent, so the executor
+// runs the solves' kernels concurrently.
+int batch_capture(sns_batch* b) {
+  cudaError_t e = cudaStreamBeginCapture(b->origin, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) return batch_fail(b, SNS_ERR_CUDA, cuda_msg("cudaStreamBeginCapture", e));
+  e = cudaEventRecord(b->fork, b->origin);
+  for (size_t i = 0; i < b->h.size() && e == cudaSuccess; ++i) {
+    cudaStream_t st = sns::handle_stream(b->h[i]);
+    e = cudaStreamWaitEvent(st, b->fork, 0);
+    if (e != cudaSuccess) break;
+    sns::enqueue_step(b->h[i], b->dt[i]);
+    e = cudaEventRecord(b->join[i], st);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(b->origin, b->join[i], 0);
+  }
+  cudaGraph_t graph = nullptr;
+  const cudaError_t e2 = cudaStreamEndCapture(b->origin, &graph);
+  if (e != cudaSuccess) {
+    if (graph) cudaGraphDestroy(graph);
+    return batch_fail(b, SNS_ERR_CUDA, cuda_msg("batch capture", e));
+  }
+  if (e2 != cudaSuccess) return batch_fail(b, SNS_ERR_CUDA, cuda_msg("cudaStreamEndCapture", e2));
+  e = cudaGraphInstantiate(&b->exec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (e != cudaSuccess) return batch_fail(b, SNS_ERR_CUDA, cuda_msg("cudaGraphInstantiate", e));
+  return SNS_OK;
+}
+
+int batch_finish(sns_batch* b, const char* what) {
+  cudaError_t e = cudaStreamSynchronize(b->origin);
+  if (e != cudaSuccess) return batch_fail(b, SNS_ERR_CUDA, cuda_msg(what, e));
+  for (sns_handle* h : b->h) {
+    const int rc = sns::finish_handle(h, what);
+    if (rc != SNS_OK) return batch_fail(b, rc, sns::handle_error(h));
+  }
+  return SNS_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------------------
+// Continuous-batching server.
+struct sns_server {
+  struct Pending {
+    int64_t id;
+    sns_request req;
+  };
+  struct Resident {
+    sns_handle* h = nullptr;
+    cudaGraphExec_t step = nullptr;  // one full step of size dt
+    int64_t id = 0;
+    sns_request req{};
+    double dt = 0.0, t = 0.0;
+    int steps = 0;
+    size_t bytes = 0;
+  };
+  size_t budget = 0, used = 0;
+  int precision = 0;
+  int device = 0;
+  int64_t next_id = 1;
+  std::deque<Pending> queue;
+  std::vector<Resident> resident;
+  std::deque<sns_result> done;  // finished, not yet returned
+  std::string err;
+};
+
+namespace {
+
+int server_fail(sns_server* s, int code, const std::string& msg) {
+  s->err = msg;
+  return code;
+}
+
+void retire(sns_server* s, size_t i) {
+  sns_server::Resident& r = s->resident[i];
+  if (r.step) cudaGraphExecDestroy(r.step);
+  if (r.h) sns_destroy(r.h);
+  s->used -= r.bytes;
+  s->resident.erase(s->resident.begin() + (long)i);
+}
+
+// Admit queued requests in arrival order while their device bytes fit the budget.
+int admit(sns_server* s) {
+  while (!s->queue.empty()) {
+    const sns_server::Pending p = s->queue.front();
+    const size_t bytes = sns_bytes_required(p.req.n, s->precision);
+    if (bytes == 0) {
+      s->queue.pop_front();
+      return server_fail(s, SNS_ERR_UNSUPPORTED, "request " + std::to_string(p.id) + ": unsupported grid size");
+    }
+    if (s->used + bytes > s->budget) {
+      if (s->resident.empty())
+        return server_fail(s, SNS_ERR_NOMEM, "request " + std::to_string(p.id) + " needs " + std::to_string(bytes) +
+                                                 " bytes, more than the whole HBM budget");
+      return SNS_OK;  // waits until memory frees up
+    }
+    sns_server::Resident r;
+    r.id = p.id;
+    r.req = p.req;
+    r.bytes = bytes;
+    int rc = sns_create(p.req.n, p.req.nu, s->precision, SNS_VISCOUS_EXPLICIT, p.req.seed, p.req.pert_amp,
+                        p.req.pert_kmax, &r.h);
+    if (rc == SNS_ERR_NOMEM && !s->resident.empty()) return SNS_OK;  // the device itself is full: wait
+    if (rc != SNS_OK) {
+      s->queue.pop_front();
+      return server_fail(s, rc, "request " + std::to_string(p.id) + ": " + sns_last_error(nullptr));
+    }
+    std::string err;
+    rc = choose_dt(r.h, p.req.n, 0.0, p.req.cfl, p.req.dt_max, &r.dt, &err);
+    if (rc == SNS_OK) rc = capture_step(r.h, r.dt, &r.step, &err);
+    if (rc != SNS_OK) {
+      sns_destroy(r.h);
+      s->queue.pop_front();
+      return server_fail(s, rc, "request " + std::to_string(p.id) + ": " + err);
+    }
+    s->queue.pop_front();
+    s->used += bytes;
+    s->resident.push_back(r);
+  }
+  return SNS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int sns_batch_create(const sns_solve_spec* specs, int count, int autotune_trials, const char* autotune_cache,
+                     sns_batch** out, double* out_dt) {
+  if (out == nullptr) return SNS_ERR_INVALID;
+  *out = nullptr;
+  if (specs == nullptr || count <= 0) {
+    sns::set_handleless_error("sns_batch_create: need at least one solve spec");
+    return SNS_ERR_INVALID;
+  }
+  sns_batch* b = new (std::nothrow) sns_batch();
+  if (b == nullptr) return SNS_ERR_NOMEM;
+  cudaGetDevice(&b->device);
+  b->h.assign(count, nullptr);
+  b->dt.assign(count, 0.0);
+  b->join.assign(count, nullptr);
+  for (int i = 0; i < count; ++i) {
+    const sns_solve_spec& sp = specs[i];
+    int rc = sns_create(sp.n, sp.nu, sp.precision, sp.viscous_mode, sp.seed, sp.pert_amp, sp.pert_kmax, &b->h[i]);
+    if (rc != SNS_OK) {
+      sns::set_handleless_error(("sns_batch_create: solve " + std::to_string(i) + ": " + sns_last_error(nullptr)).c_str());
+      batch_release(b);
+      return rc;
+    }
+    std::string err;
+    rc = choose_dt(b->h[i], sp.n, sp.dt, sp.cfl, sp.dt_max, &b->dt[i], &err);
+    if (rc != SNS_OK) {
+      sns::set_handleless_error(("sns_batch_create: solve " + std::to_string(i) + ": " + err).c_str());
+      batch_release(b);
+      return rc;
+    }
+    if (out_dt) out_dt[i] = b->dt[i];
+  }
+  if (autotune_trials > 0) {
+    // one launch-shape search per distinct (N, precision), on a scratch handle so the
+    // batch's own states are untouched by the trial steps; every member then runs it
+    std::map<std::pair<int, int>, std::array<int, 3>> shapes;
+    for (int i = 0; i < count; ++i) {
+      const auto key = std::make_pair(specs[i].n, specs[i].precision);
+      auto it = shapes.find(key);
+      if (it == shapes.end()) {
+        sns_handle* scratch = nullptr;
+        int rc = sns_create(specs[i].n, specs[i].nu, specs[i].precision, specs[i].viscous_mode, 0, 0.0, 0, &scratch);
+        std::array<int, 3> cfg{};
+        if (rc == SNS_OK) {
+          rc = sns_autotune(scratch, autotune_trials, autotune_cache, cfg.data());
+          if (rc != SNS_OK) sns::set_handleless_error(sns_last_error(scratch));
+          sns_destroy(scratch);
+        }
+        if (rc != SNS_OK) {
+          batch_release(b);
+          return rc;
+        }
+        it = shapes.emplace(key, cfg).first;
+      }
+      sns::set_launch_shape(b->h[i], it->second.data());
+    }
+  }
+  cudaError_t e = cudaStreamCreateWithFlags(&b->origin, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming);
+  for (int i = 0; i < count && e == cudaSuccess; ++i) e = cudaEventCreateWithFlags(&b->join[i], cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreate(&b->ev0);
+  if (e == cudaSuccess) e = cudaEventCreate(&b->ev1);
+  if (e != cudaSuccess) {
+    sns::set_handleless_error(cuda_msg("sns_batch_create", e).c_str());
+    batch_release(b);
+    return SNS_ERR_CUDA;
+  }
+  const int rc = batch_capture(b);
+  if (rc != SNS_OK) {
+    sns::set_handleless_error(("sns_batch_create: " + b->err).c_str());
+    batch_release(b);
+    return rc;
+  }
+  *out = b;
+  return SNS_OK;
+}
+
+int sns_batch_destroy(sns_batch* b) {
+  if (b == nullptr) return SNS_ERR_INVALID;
+  batch_release(b);
+  return SNS_OK;
+}
+
+int sns_batch_step(sns_batch* b, int nsteps) {
+  if (b == nullptr) return SNS_ERR_INVALID;
+  if (nsteps < 0) return batch_fail(b, SNS_ERR_INVALID, "negative step count");
+  cudaSetDevice(b->device);
+  for (int k = 0; k < nsteps; ++k) {
+    const cudaError_t e = cudaGraphLaunch(b->exec, b->origin);
+    if (e != cudaSuccess) return batch_fail(b, SNS_ERR_CUDA, cuda_msg("cudaGraphLaunch", e));
+  }
+  return batch_finish(b, "sns_batch_step");
+}
+
+int sns_batch_time_steps(sns_batch* b, int nsteps, double* elapsed_ms) {
+  if (b == nullptr) return SNS_ERR_INVALID;
+  if (nsteps < 0 || elapsed_ms == nullptr) return batch_fail(b, SNS_ERR_INVALID, "invalid argument");
+  cudaSetDevice(b->device);
+  cudaError_t e = cudaEventRecord(b->ev0, b->origin);
+  for (int k = 0; k < nsteps && e == cudaSuccess; ++k) e = cudaGraphLaunch(b->exec, b->origin);
+  if (e == cudaSuccess) e = cudaEventRecord(b->ev1, b->origin);
+  if (e != cudaSuccess) return batch_fail(b, SNS_ERR_CUDA, cuda_msg("sns_batch_time_steps", e));
+  const int rc = batch_finish(b, "sns_batch_time_steps");
+  if (rc != SNS_OK) return rc;
+  float ms = 0.f;
+  e = cudaEventElapsedTime(&ms, b->ev0, b->ev1);
+  if (e != cudaSuccess) return batch_fail(b, SNS_ERR_CUDA, cuda_msg("cudaEventElapsedTime", e));
+  *elapsed_ms = ms;
+  return SNS_OK;
+}
+
+sns_handle* sns_batch_handle(sns_batch* b, int i) {
+  if (b == nullptr || i < 0 || i >= (int)b->h.size()) return nullptr;
+  return b->h[i];
+}
+
+int sns_batch_size(const sns_batch* b) { return b ? (int)b->h.size() : 0; }
+
+const char* sns_batch_last_error(const sns_batch* b) { return b ? b->err.c_str() : ""; }
+
+int sns_server_create(size_t hbm_budget_bytes, int precision, sns_server** out) {
+  if (out == nullptr) return SNS_ERR_INVALID;
+  *out = nullptr;
+  if (hbm_budget_bytes == 0 || sns_bytes_required(64, precision) == 0) {
+    sns::set_handleless_error("sns_server_create: need a positive budget and a known precision");
+    return SNS_ERR_INVALID;
+  }
+  sns_server* s = new (std::nothrow) sns_server();
+  if (s == nullptr) return SNS_ERR_NOMEM;
+  s->budget = hbm_budget_bytes;
+  s->precision = precision;
+  cudaGetDevice(&s->device);
+  *out = s;
+  return SNS_OK;
+}
+
+int sns_server_destroy(sns_server* s) {
+  if (s == nullptr) return SNS_ERR_INVALID;
+  cudaSetDevice(s->device);
+  while (!s->resident.empty()) retire(s, s->resident.size() - 1);
+  delete s;
+  return SNS_OK;
+}
+
+int sns_server_submit(sns_server* s, const sns_request* r, int64_t* out_id) {
+  if (s == nullptr) return SNS_ERR_INVALID;
+  if (r == nullptr || !(r->t_end > 0.0) || !(r->nu >= 0.0) || r->n <= 0)
+    return server_fail(s, SNS_ERR_INVALID, "request needs n > 0, nu >= 0 and t_end > 0");
+  if (sns_bytes_required(r->n, s->precision) == 0) return server_fail(s, SNS_ERR_UNSUPPORTED, "unsupported request");
+  const int64_t id = s->next_id++;
+  s->queue.push_back({id, *r});
+  if (out_id) *out_id = id;
+  return SNS_OK;
+}
+
+int sns_server_step(sns_server* s, sns_result* done, int max_done, int* ndone, int* resident, int* queued,
+                    size_t* bytes_in_use) {
+  if (s == nullptr) return SNS_ERR_INVALID;
+  if (ndone) *ndone = 0;
+  cudaSetDevice(s->device);
+  int rc = admit(s);
+  if (rc != SNS_OK) return rc;
+  // One tick: every resident solve advances on its own stream, the largest by one step and
+  // smaller ones by proportionally more (N_max^3 / N^3 steps, at most kMaxTickSteps), so a
+  // small solve is not held to the pace of the largest.  A full step replays the solve's
+  // graph; the last one (clipped to the horizon) is launched directly.
+  constexpr double kMaxTickSteps = 64.0;
+  double wmax = 0.0;
+  for (const sns_server::Resident& r : s->resident) wmax = std::fmax(wmax, std::pow((double)r.req.n, 3.0));
+  for (sns_server::Resident& r : s->resident) {
+    const int k = (int)std::fmin(kMaxTickSteps, std::fmax(1.0, std::floor(wmax / std::pow((double)r.req.n, 3.0))));
+    for (int j = 0; j < k && r.t < r.req.t_end - 1.0e-12 * r.req.t_end; ++j) {
+      const double left = r.req.t_end - r.t;
+      if (left >= r.dt - 1.0e-14 * r.req.t_end) {
+        const cudaError_t e = cudaGraphLaunch(r.step, sns::handle_stream(r.h));
+        if (e != cudaSuccess) return server_fail(s, SNS_ERR_CUDA, cuda_msg("cudaGraphLaunch", e));
+        r.t += r.dt;
+      } else {
+        sns::enqueue_step(r.h, left);
+        r.t = r.req.t_end;
+      }
+      ++r.steps;
+    }
+  }
+  for (size_t i = 0; i < s->resident.size(); ++i) {
+    rc = sns::finish_handle(s->resident[i].h, "sns_server_step");
+    if (rc != SNS_OK) return server_fail(s, rc, sns::handle_error(s->resident[i].h));
+  }
+  // retire the solves that reached their horizon
+  for (size_t i = s->resident.size(); i-- > 0;) {
+    sns_server::Resident& r = s->resident[i];
+    if (r.t < r.req.t_end - 1.0e-12 * r.req.t_end) continue;
+    sns_result res{};
+    res.id = r.id;
+    res.n = r.req.n;
+    res.steps = r.steps;
+    res.dt = r.dt;
+    rc = sns_diagnostics(r.h, r.req.t_end, &res.final);
+    if (rc != SNS_OK) return server_fail(s, rc, sns_last_error(r.h));
+    s->done.push_back(res);
+    retire(s, i);
+  }
+  int nd = 0;
+  while (!s->done.empty() && nd < max_done && done != nullptr) {
+    done[nd++] = s->done.front();
+    s->done.pop_front();
+  }
+  if (ndone) *ndone = nd;
+  if (resident) *resident = (int)s->resident.size();
+  if (queued) *queued = (int)s->queue.size();
+  if (bytes_in_use) *bytes_in_use = s->used;
+  return SNS_OK;
+}
+
+const char* sns_server_last_error(const sns_server* s) { return s ? s->err.c_str() : ""; }
+
+}  // extern "C"

@@ -1,5 +1,6 @@
 // Command-line driver: the reference's flags (src/main_ava.cpp:43-73) plus
-// --seed --pert-amp --pert-kmax --dump-final --precision fp64|fp32 --viscous explicit|if.
+// --seed --pert-amp --pert-kmax --dump-final --precision fp64|fp32 --viscous explicit|if
+// --checkpoint-every K --restart PATH.
 #include "spectral/ava_taylor_green.hpp"
 
 #include <algorithm>
@@ -56,6 +57,8 @@ int main(int argc, char** argv) {
     const std::string visc = string_arg(argc, argv, "--viscous", "explicit");
     if (visc != "explicit" && visc != "if") throw std::runtime_error("--viscous must be explicit or if");
     c.viscous_mode = visc == "if" ? 1 : 0;
+    c.checkpoint_every = int_arg(argc, argv, "--checkpoint-every", 0);
+    c.restart = string_arg(argc, argv, "--restart", "");
     spectral::ava_solver::run_taylor_green(c);
   } catch (const std::exception& e) {
     std::cerr << "error: " << e.what() << "\n";

@@ -33,11 +33,12 @@ double wall() {
 struct TaylorGreenSolver::Impl {
   sns_handle* h = nullptr;
   int n = 0;
+  int precision = 0;
   double step_time = 0.0, diagnostics_time = 0.0, max_velocity_time = 0.0;
   long long step_calls = 0, diagnostics_calls = 0, max_velocity_calls = 0;
 
-  Impl(int n_in, double reynolds, std::uint64_t seed, double amp, int kmax, int precision, int viscous_mode)
-      : n(n_in) {
+  Impl(int n_in, double reynolds, std::uint64_t seed, double amp, int kmax, int precision_in, int viscous_mode)
+      : n(n_in), precision(precision_in) {
     if (n <= 0) throw std::runtime_error("grid size must be positive");
     if (reynolds <= 0.0) throw std::runtime_error("Reynolds number must be positive");
     const int rc = sns_create(n, 1.0 / reynolds, precision, viscous_mode, seed, amp, kmax, &h);
@@ -120,23 +121,89 @@ void TaylorGreenSolver::dump_velocity(const std::string& path) {
   f.write(reinterpret_cast<const char*>(buf.data()), static_cast<std::streamsize>(buf.size() * sizeof(double)));
 }
 
+void TaylorGreenSolver::save_checkpoint(const std::string& path, double t, long long step) {
+  const int n = impl_->n;
+  const std::size_t full = static_cast<std::size_t>(n) * n * n;
+  const std::size_t nh = static_cast<std::size_t>(n / 2 + 1);
+  std::vector<double> buf(3 * 2 * full);
+  double* st[3] = {buf.data(), buf.data() + 2 * full, buf.data() + 4 * full};
+  impl_->check(sns_get_state(impl_->h, st), "TaylorGreenSolver::save_checkpoint");
+  std::ofstream f(path + ".tmp", std::ios::binary);
+  if (!f) throw std::runtime_error("cannot write " + path);
+  const char magic[8] = {'S', 'N', 'S', 'C', 'K', 'P', 'T', '1'};
+  const std::int64_t hdr[2] = {n, impl_->precision};
+  const std::int64_t step64 = step;
+  f.write(magic, 8);
+  f.write(reinterpret_cast<const char*>(hdr), sizeof hdr);
+  f.write(reinterpret_cast<const char*>(&t), sizeof t);
+  f.write(reinterpret_cast<const char*>(&step64), sizeof step64);
+  for (int c = 0; c < 3; ++c)
+    for (std::size_t row = 0; row < static_cast<std::size_t>(n) * n; ++row)
+      f.write(reinterpret_cast<const char*>(st[c] + 2 * row * n), static_cast<std::streamsize>(2 * nh * sizeof(double)));
+  f.close();
+  if (!f) throw std::runtime_error("write failed: " + path);
+  std::filesystem::rename(path + ".tmp", path);  // a crash mid-write leaves the old checkpoint
+}
+
+void TaylorGreenSolver::load_checkpoint(const std::string& path, double* t, long long* step) {
+  const int n = impl_->n;
+  std::ifstream f(path, std::ios::binary);
+  if (!f) throw std::runtime_error("cannot read " + path);
+  char magic[8];
+  std::int64_t hdr[2] = {0, 0}, step64 = 0;
+  double t0 = 0.0;
+  f.read(magic, 8);
+  f.read(reinterpret_cast<char*>(hdr), sizeof hdr);
+  f.read(reinterpret_cast<char*>(&t0), sizeof t0);
+  f.read(reinterpret_cast<char*>(&step64), sizeof step64);
+  if (!f || std::string(magic, 8) != "SNSCKPT1") throw std::runtime_error(path + " is not a checkpoint");
+  if (hdr[0] != n) throw std::runtime_error(path + ": grid " + std::to_string(hdr[0]) + " != " + std::to_string(n));
+  const std::size_t full = static_cast<std::size_t>(n) * n * n;
+  const std::size_t nh = static_cast<std::size_t>(n / 2 + 1);
+  std::vector<double> buf(3 * 2 * full, 0.0);
+  double* st[3] = {buf.data(), buf.data() + 2 * full, buf.data() + 4 * full};
+  for (int c = 0; c < 3; ++c)
+    for (std::size_t row = 0; row < static_cast<std::size_t>(n) * n; ++row)
+      f.read(reinterpret_cast<char*>(st[c] + 2 * row * n), static_cast<std::streamsize>(2 * nh * sizeof(double)));
+  if (!f) throw std::runtime_error(path + ": truncated checkpoint");
+  // the state stores mx in [0, n/2]; set_state reads only those columns of the full layout
+  const double* cst[3] = {st[0], st[1], st[2]};
+  impl_->check(sns_set_state(impl_->h, cst), "TaylorGreenSolver::load_checkpoint");
+  *t = t0;
+  *step = step64;
+}
+
 void run_taylor_green(const RunConfig& config) {
   if (config.dt <= 0.0 || config.cfl <= 0.0 || config.output_dt <= 0.0)
     throw std::runtime_error("--dt, --cfl, and --output-dt must be positive");
   std::filesystem::create_directories(config.output_dir);
   const std::string csv_path = config.output_dir + "/taylor_green_diagnostics.csv";
-  std::ofstream csv(csv_path);
+  const std::string ckpt_path = config.output_dir + "/checkpoint.bin";
+  const bool resume = !config.restart.empty();
+  std::ofstream csv(csv_path, resume ? std::ios::app : std::ios::trunc);
   csv << std::setprecision(17);
-  csv << "t,kinetic_energy,dissipation,enstrophy,max_spectral_divergence,max_velocity,dt,cfl,main_dt,main_cfl\n";
+  if (!resume)
+    csv << "t,kinetic_energy,dissipation,enstrophy,max_spectral_divergence,max_velocity,dt,cfl,main_dt,main_cfl\n";
 
   const double init_t0 = wall();
   TaylorGreenSolver solver(config.n, config.reynolds, config.seed, config.pert_amp, config.pert_kmax, config.precision,
                            config.viscous_mode);
+  double t = 0.0;
+  int step = 0;
+  if (resume) {
+    long long s0 = 0;
+    solver.load_checkpoint(config.restart, &t, &s0);
+    step = static_cast<int>(s0);
+    std::cout << "resumed from " << config.restart << " at step " << step << " t=" << t << "\n";
+  }
+  const int first_step = step;
+  auto checkpoint = [&](int s) {
+    if (config.checkpoint_every > 0 && s > first_step && s % config.checkpoint_every == 0)
+      solver.save_checkpoint(ckpt_path, t, s);
+  };
   const double init_time = wall() - init_t0;
   const double run_t0 = wall();
   const double dx = 2.0 * kPi / static_cast<double>(config.n);
-  double t = 0.0;
-  int step = 0;
   int output_count = 0;
   auto write_row = [&](double time, bool force_print, double last_dt, double last_cfl, double main_dt,
                        double main_cfl) {
@@ -155,8 +222,12 @@ void run_taylor_green(const RunConfig& config) {
 
   if (config.adaptive_cfl) {
     double next_output = 0.0;
-    write_row(t, true, 0.0, 0.0, 0.0, 0.0);
-    next_output += config.output_dt;
+    if (!resume) {
+      write_row(t, true, 0.0, 0.0, 0.0, 0.0);
+      next_output += config.output_dt;
+    } else {
+      while (next_output <= t + 1.0e-12) next_output += config.output_dt;
+    }
     while (t < config.t_end - 1.0e-14) {
       if (step >= config.max_steps)
         throw std::runtime_error("adaptive CFL run exceeded --max-steps before reaching --t-end");
@@ -178,9 +249,11 @@ void run_taylor_green(const RunConfig& config) {
         write_row(t, t >= config.t_end - 1.0e-12, dt_step, actual_cfl, main_dt, main_cfl);
         while (next_output <= t + 1.0e-12) next_output += config.output_dt;
       }
+      checkpoint(step);
     }
   } else {
-    for (step = 0; step <= config.steps; ++step) {
+    for (; step <= config.steps; ++step) {
+      checkpoint(step);
       if (step % config.output_every == 0 || step == config.steps) {
         const bool first = step == 0;
         const double fixed_cfl = solver.max_velocity() * config.dt / dx;

@@ -110,7 +110,7 @@ def test_steps_match_oracle(Solver, n):
     assert rel_l2(u, [half_to_full(c) for c in o.u_hat]) < 1e-12
 
 
-@pytest.mark.parametrize("n", [12, 64])
+@pytest.mark.parametrize("n", [12, 48, 64, 96, 128])
 def test_diagnostics_match_oracle(Solver, n):
     o = oracle_state(n, 9, 3e-2, max(1, min(5, n // 2 - 1)))
     with Solver(n, 1600.0, seed=9, pert_amp=3e-2, pert_kmax=max(1, min(5, n // 2 - 1))) as s:

@@ -60,6 +60,24 @@ def test_fp32_rhs_matches_oracle(Solver, n):
     assert rel_l2(r, r_ref) < 2e-5
 
 
+@pytest.mark.parametrize("n", [32, 48, 96, 128])
+def test_fp32_diagnostics_match_oracle(Solver, n):
+    """Energy, enstrophy, dissipation and vmax of an FP32 state against the FP64 oracle
+    (the FP32 rounding of the state bounds the relative error: 1e-6)."""
+    o = TaylorGreenR2C(n, 1600.0)
+    p = perturbation_half(n, 9, 3e-2, max(1, min(5, n // 2 - 1)))
+    for c in range(3):
+        o.u_hat[c] = o.u_hat[c] + p[c]
+    o.project_truncate(o.u_hat)
+    with Solver(n, 1600.0, seed=9, pert_amp=3e-2, pert_kmax=max(1, min(5, n // 2 - 1)), precision=FP32) as s:
+        d = s.diagnostics(0.0)
+        vmax = s.max_velocity()
+    dr = o.diagnostics(0.0)
+    for key in ("kinetic_energy", "dissipation", "enstrophy", "max_velocity"):
+        assert abs(d[key] - dr[key]) <= 1e-6 * abs(dr[key]), key
+    assert abs(vmax - dr["max_velocity"]) <= 1e-6 * dr["max_velocity"]
+
+
 @pytest.mark.parametrize("n,dt,steps,amp", [(64, 5e-3, 200, 0.0), (128, 2.5e-3, 100, 1e-3), (256, 2.5e-3, 40, 1e-3)])
 def test_fp32_trajectory_vs_fp64(Solver, n, dt, steps, amp):
     kmax = 8 if amp else 0
