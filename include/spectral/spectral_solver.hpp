@@ -83,6 +83,16 @@ class SpectralNavierStokes {
   double dissipation(const VectorSpectral& u_hat);
   double max_spectral_divergence(const VectorSpectral& u_hat) const;
   Diagnostics diagnostics(const VectorSpectral& u_hat, double t);
+
+  // Device-resident overloads (additions to the reference's interface): the host-vector
+  // methods above copy the state to the GPU and back on every call; these keep it in HBM
+  // between calls.  load_state uploads once, step_rk3(dt, nsteps) advances on the device,
+  // diagnostics(t) reads one row, state() downloads on demand.
+  void load_state(const VectorSpectral& u_hat);
+  void step_rk3(double dt, int nsteps = 1);
+  Diagnostics diagnostics(double t);
+  VectorSpectral state();
+
   void reset_profile();
   const SolverProfile& profile() const { return profile_; }
 

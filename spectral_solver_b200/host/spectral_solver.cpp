@@ -245,6 +245,37 @@ Diagnostics SpectralNavierStokes::diagnostics(const VectorSpectral& u_hat, doubl
   return row;
 }
 
+void SpectralNavierStokes::load_state(const VectorSpectral& u_hat) {
+  sns_handle* h = solver_handle();
+  const double* in[3] = {u_hat[0].data(), u_hat[1].data(), u_hat[2].data()};
+  check(sns_set_state(h, in), h, "SpectralNavierStokes::load_state");
+}
+
+void SpectralNavierStokes::step_rk3(double dt, int nsteps) {
+  const auto t0 = Clock::now();
+  sns_handle* h = solver_handle();
+  check(sns_step(h, dt, nsteps), h, "SpectralNavierStokes::step_rk3");
+  profile_.steps += nsteps;
+  profile_.step_rk3 += seconds_since(t0);
+}
+
+Diagnostics SpectralNavierStokes::diagnostics(double t) {
+  const auto t0 = Clock::now();
+  sns_handle* h = solver_handle();
+  sns_diag d{};
+  check(sns_diagnostics(h, t, &d), h, "SpectralNavierStokes::diagnostics");
+  profile_.diagnostics += seconds_since(t0);
+  return Diagnostics{t, d.kinetic_energy, 2.0 * nu_ * d.enstrophy, d.enstrophy, d.max_spectral_divergence};
+}
+
+VectorSpectral SpectralNavierStokes::state() {
+  sns_handle* h = solver_handle();
+  VectorSpectral out = zeros_spectral(fft_.spectral_storage_size());
+  double* o[3] = {out[0].data(), out[1].data(), out[2].data()};
+  check(sns_get_state(h, o), h, "SpectralNavierStokes::state");
+  return out;
+}
+
 void SpectralNavierStokes::reset_profile() { profile_ = SolverProfile{}; }
 
 bool SpectralNavierStokes::keep_mode(const SpectralMode& m) const {

@@ -153,7 +153,8 @@ def test_checkpoint_resume_is_exact(tmp_path, adaptive, precision):
     flags = ["--n", "48", "--re", "800", "--seed", "3", "--pert-amp", "1e-3", "--pert-kmax", "6",
              "--precision", precision]
     if adaptive:
-        flags += ["--adaptive-cfl", "1", "--dt", "0.5", "--cfl", "0.5", "--t-end", "1.0", "--output-dt", "0.1"]
+        # the 0.02 cap sets every step (the CFL step is ~0.065): 20 steps reach t = 0.4
+        flags += ["--adaptive-cfl", "1", "--dt", "0.02", "--cfl", "0.5", "--t-end", "1.0", "--output-dt", "0.1"]
     else:
         flags += ["--adaptive-cfl", "0", "--dt", "0.01", "--steps", "40", "--output-every", "5"]
     full, _ = run_cli(flags, tmp_path / "full")
