@@ -52,8 +52,9 @@ LAUNCHES_PER_STEP = 3 * 6
 TRAFFIC_PER_POINT = {"p5_sweep": 3.262e9 / 256 ** 3, "p3_xpass": 2.445e9 / 256 ** 3,
                      "p4_yfwd": 3.268e9 / 256 ** 3, "p1_zinv_phase": 1.166e9 / 256 ** 3,
                      "p2_yinv": 1.582e9 / 256 ** 3}
-# The same for the FP32 precision form (filled from its own captures).
-TRAFFIC_PER_POINT_FP32 = {}
+# The same for the FP32 precision form (profiles/k_p5_xpass2_256_fp32.txt: single-launch
+# captures at 256^3, scaled by N^3 like the FP64 figures).
+TRAFFIC_PER_POINT_FP32 = {"p3_xpass": (0.465e9 + 0.773e9) / 256 ** 3, "p5_sweep": (1.271e9 + 0.382e9) / 256 ** 3}
 
 
 def load_peaks():

@@ -428,12 +428,15 @@ struct XP {
   static constexpr int M = N / 16;                 // stage-B radix
   static constexpr bool PAIR = (M == 32);          // radix 32 as two radix-16 halves + shuffle
   static constexpr int NH = N / 2;
-  static constexpr int ROWS = (N == 256) ? 2 : 1;  // rows per iteration (192 threads busy)
+  // rows per iteration: two where their staging fits the CTA budget (N = 256; N = 512 in
+  // FP32), so the inverse stages keep all 192 threads busy and one barrier sequence serves
+  // two rows
+  static constexpr int ROWS = (N == 256 || sizeof(C) == 8) ? 2 : 1;
   static constexpr int SP = N + N / 16;            // padded sequence (one slot per 16)
   static constexpr int NT = 192;
   // resident CTAs per SM the register budget is built for: the FP32 rows are half the
   // shared memory, so three CTAs fit where FP64 fits two
-  static constexpr int MINB = sizeof(C) == 8 ? 3 : 2;
+  static constexpr int MINB = (sizeof(C) == 8 && N == 256) ? 3 : 2;
   // staged row of one field: NH + 1 values rounded up to 16 bytes (the bulk-copy unit)
   static constexpr int RS = (int)(((NH + 1) * sizeof(C) + 15) / 16 * 16 / sizeof(C));
   static constexpr int ROWIN = 6 * RS;
@@ -551,9 +554,9 @@ k_xpass2(C* __restrict__ work, const C* __restrict__ unyq, const C* __restrict__
 
     // ---- inverse stage B: z_c into the staging buffer (its inputs are consumed)
     if constexpr (X::PAIR) {
-      if (tid < 96) {
-        const int lane = tid & 31, c = tid >> 5, j = lane & 15, h = lane >> 4;
-        const C* Wc = W + c * SP;
+      if (tid < ROWS * 96) {
+        const int lane = tid & 31, c = (tid >> 5) % 3, r = tid / 96, j = lane & 15, h = lane >> 4;
+        const C* Wc = W + (r * 6 + c) * SP;
         C v[16];
 #pragma unroll
         for (int i = 0; i < 16; ++i) {
@@ -565,7 +568,7 @@ k_xpass2(C* __restrict__ work, const C* __restrict__ unyq, const C* __restrict__
 #pragma unroll
           for (int q = 1; q < 16; ++q) v[q] = cmulc(v[q], tw2[16 * 16 + q]);  // conj W32^q
         }
-        C* Zc = S + c * SP;
+        C* Zc = S + r * STG + c * SP;
 #pragma unroll
         for (int q = 0; q < 16; ++q) {
           const C o = shfl2_xor(v[q], 16);
@@ -589,8 +592,10 @@ k_xpass2(C* __restrict__ work, const C* __restrict__ unyq, const C* __restrict__
     __syncthreads();
 
     // ---- forward stage A: products fused into the loads
-    {
-      const int t = tid % M, ab = (tid / M) % 6, r = tid / (6 * M);
+    constexpr int FWD_ROWS = X::NT / (6 * M);  // rows one pass of the CTA covers
+#pragma unroll 1
+    for (int r0 = 0; r0 < ROWS; r0 += FWD_ROWS) {
+      const int t = tid % M, ab = (tid / M) % 6, r = r0 + tid / (6 * M);
       // pairs 00 01 02 11 12 22
       const int ca = (ab >= 3) + (ab >= 5), cb = ab < 3 ? ab : (ab < 5 ? ab - 2 : 2);
       const C* Za = S + r * STG + ca * SP;
@@ -611,8 +616,10 @@ k_xpass2(C* __restrict__ work, const C* __restrict__ unyq, const C* __restrict__
 
     // ---- forward stage B, r2c unpack through the partner lane, stores to HBM
     if constexpr (X::PAIR) {
+#pragma unroll 1
+     for (int r = 0; r < ROWS; ++r) {
       const int lane = tid & 31, ab = tid >> 5, j = lane & 15, h = lane >> 4;
-      const C* Wp = W + ab * SP;
+      const C* Wp = W + (r * 6 + ab) * SP;
       C v[16];
 #pragma unroll
       for (int i = 0; i < 16; ++i) {
@@ -630,7 +637,7 @@ k_xpass2(C* __restrict__ work, const C* __restrict__ unyq, const C* __restrict__
         v[q] = h ? csub(o, v[q]) : cadd(v[q], o);  // X(j + 16 (q + 16 h))
       }
       const int partner = ((16 - j) & 15) + 16 * (1 - h);
-      const long long row = it;
+      const long long row = it * ROWS + r;
       C* o0 = work + (long long)(2 * ab) * g.field + row * g.pitch;
       C* o1 = o0 + g.field;
 #pragma unroll
@@ -650,6 +657,7 @@ k_xpass2(C* __restrict__ work, const C* __restrict__ unyq, const C* __restrict__
           }
         }
       }
+     }
     } else {
       const int j = tid & 15, sq = tid >> 4, r = sq / 6, ab = sq % 6;
       const C* Wp = W + (r * 6 + ab) * SP;
@@ -1492,7 +1500,12 @@ __global__ void __launch_bounds__(256) k_reduce(const double* __restrict__ parti
 // Host launchers.
 template <class K>
 static void set_smem(K kernel, size_t bytes) {
-  if (bytes > 48 * 1024) cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (bytes > 48 * 1024) {
+    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    // prefer the largest shared-memory carveout so the occupancy the launch shapes are
+    // computed from (and get) is bounded by the real budget, not a smaller default split
+    cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, (int)cudaSharedmemCarveoutMaxShared);
+  }
 }
 
 template <int N, class C>

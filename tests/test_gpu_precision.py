@@ -99,3 +99,19 @@ def test_fp32_trajectory_vs_fp64(Solver, n, dt, steps, amp):
     print(f"N={n}: max|dE|={worst_e:.3e} max|d eps|={worst_eps:.3e} velocity rel L2={rel_l2(u32, u64):.3e}")
     assert worst_e <= 1e-6 and worst_eps <= 1e-6
     assert rel_l2(u32, u64) < 1e-4
+
+
+def test_fp32_512_steps_track_fp64(Solver):
+    """The 512^3 kernels of the precision form (two-row x pass, fused P5) against the FP64
+    form: both from the analytic field, 20 steps, E and eps within 1e-6."""
+    n, dt = 512, 1e-3
+    with Solver(n, 1600.0, precision=FP32) as s32:
+        s32.step(dt, 20)
+        d32 = s32.diagnostics(20 * dt)
+    with Solver(n, 1600.0) as s64:
+        s64.step(dt, 20)
+        d64 = s64.diagnostics(20 * dt)
+    assert abs(d32["kinetic_energy"] - d64["kinetic_energy"]) <= 1e-6
+    assert abs(d32["dissipation"] - d64["dissipation"]) <= 1e-6
+    assert abs(d32["enstrophy"] - d64["enstrophy"]) <= 1e-6 * d64["enstrophy"] * 10
+    assert d32["max_spectral_divergence"] < 1e-7 * n ** 3
