@@ -21,6 +21,7 @@
 #include "sns_kernels.cuh"
 #include "sns_tma.cuh"
 
+#include <algorithm>
 #include <cstdio>
 
 namespace sns {
@@ -1569,14 +1570,26 @@ struct Launch {
     }
   }
   // Persistent grid of the fused P5 (0: this size runs forward z + sweep as two kernels).
+  // The runtime's occupancy query reports one CTA per SM for this tensor-memory kernel
+  // whatever its allocation, so residency is computed from the kernel's own limits: shared
+  // memory, registers, threads, and its tensor-memory columns (512 per SM).
   static int p5_grid(int nsm) {
     if constexpr (N == 128 || N == 256 || N == 512) {
-      int nb = 0;
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_p5<N, C>, nt_p5<N>(), tma_smem<N, C>());
-      // tensor memory holds at most 512 columns per SM
-      const int cap = 512 / (int)p5_cols<N>();
-      nb = nb < 1 ? 1 : (nb > cap ? cap : nb);
-      return nsm * nb;
+      int dev = 0, smem_sm = 0, smem_rsv = 0, regs_sm = 0, thr_sm = 0;
+      cudaGetDevice(&dev);
+      cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+      cudaDeviceGetAttribute(&smem_rsv, cudaDevAttrReservedSharedMemoryPerBlock, dev);
+      cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev);
+      cudaDeviceGetAttribute(&thr_sm, cudaDevAttrMaxThreadsPerMultiProcessor, dev);
+      cudaFuncAttributes fa{};
+      cudaFuncGetAttributes(&fa, k_p5<N, C>);
+      const long long smem_cta = (long long)tma_smem<N, C>() + fa.sharedSizeBytes + smem_rsv;
+      const long long regs_cta = (long long)((fa.numRegs + 7) / 8 * 8) * nt_p5<N>();
+      int nb = 512 / (int)p5_cols<N>();
+      if (smem_cta > 0) nb = (int)std::min<long long>(nb, smem_sm / smem_cta);
+      if (regs_cta > 0) nb = (int)std::min<long long>(nb, regs_sm / regs_cta);
+      nb = std::min(nb, thr_sm / nt_p5<N>());
+      return nsm * (nb < 1 ? 1 : nb);
     } else {
       (void)nsm;
       return 0;
