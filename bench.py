@@ -117,7 +117,9 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
-def dist_setup(args):
+def dist_setup(args, backend: str = "nccl"):
+    """One process per GPU (torchrun's env).  The process group carries only the barriers
+    and the max-over-ranks timing: the replicas share no data."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -126,13 +128,27 @@ def dist_setup(args):
         import datetime
         import torch
         import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
         pg = dist
     return world, rank, local, pg
 
 
+def _reduce_device(pg):
+    return "cuda" if pg.get_backend() == "nccl" else "cpu"
+
+
+def replica_rate(world: int, n: int, steps: int, ms_max: float) -> float:
+    """Whole-job Gpt*RK3-steps/s of `world` replicas of an N^3 solve: every rank stepped
+    its own grid `steps` times; the slowest rank's device time is the job's time."""
+    return world * n ** 3 * steps / (ms_max / 1e3) / 1e9
+
+
 def barrier_sync(pg):
+    if pg is not None and _reduce_device(pg) == "cpu":
+        pg.barrier()
+        return
     import torch
     torch.cuda.synchronize()
     if pg is not None:
@@ -144,7 +160,7 @@ def max_over_ranks(pg, value: float) -> float:
     if pg is None:
         return value
     import torch
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    t = torch.tensor([value], dtype=torch.float64, device=_reduce_device(pg))
     pg.all_reduce(t, op=pg.ReduceOp.MAX)
     return float(t.item())
 
@@ -217,8 +233,7 @@ def measure_form(args, n, precision, local, pg):
     clocks = clk.summary()
     ms_max = max_over_ranks(pg, ms)
     world = int(os.environ.get("WORLD_SIZE", "1"))
-    units = world * n ** 3 * args.steps
-    value = units / (ms_max / 1e3) / 1e9
+    value = replica_rate(world, n, args.steps, ms_max)
     # Per-pass device times (events between passes, separate from the timed region).
     prof = s.profile_passes(DT, 1)
     w = 8 if precision == 0 else 4

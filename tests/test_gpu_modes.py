@@ -78,3 +78,23 @@ def test_if_deviation_from_explicit_scheme(Solver):
           f"dE/E {abs(di['kinetic_energy'] - de['kinetic_energy']) / de['kinetic_energy']:.3e}")
     assert 0.0 < dev < 1e-6
     assert abs(di["kinetic_energy"] - de["kinetic_energy"]) <= 1e-8 * de["kinetic_energy"]
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_inviscid_time_reversibility(Solver, precision):
+    """The reference's inviscid reversibility benchmark (its method notes, section 18): nu = 0,
+    integrate forward, reverse time, integrate back; E and enstrophy return to their initial
+    values up to the time-stepping error.  The oracle's run of the same schedule at 64^3
+    recovers E and enstrophy to 6.7e-10 (RK3 truncation, dt = 5e-3); the bound keeps 10x
+    margin, and the FP32 form's round-off sets its own bound."""
+    n, dt, steps = 64, 5e-3, 200
+    with Solver(n, nu=0.0, precision=precision) as s:
+        d0 = s.diagnostics(0.0)
+        s.step(dt, steps)
+        d1 = s.diagnostics(dt * steps)
+        s.step(-dt, steps)
+        d2 = s.diagnostics(0.0)
+    assert d1["enstrophy"] > 1.1 * d0["enstrophy"]  # the flow did evolve
+    tol = 7e-9 if precision == 0 else 1e-5
+    for key in ("kinetic_energy", "enstrophy"):
+        assert abs(d2[key] - d0[key]) <= tol * d0[key], (key, d0[key], d2[key])
