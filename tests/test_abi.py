@@ -60,6 +60,26 @@ def test_null_handle_calls(lib):
     assert lib.sns_debug_fail_after(None, 1) == 1
     assert lib.sns_set_viscosity(None, 1.0) == 1
     assert lib.sns_grid_size(None) == 0
+    assert lib.sns_autotune(None, 1, None, None) == 1
+    assert lib.sns_batch_step(None, 1) == 1
+    assert lib.sns_batch_destroy(None) == 1
+    assert lib.sns_batch_size(None) == 0
+    assert lib.sns_batch_handle(None, 0) is None
+    assert lib.sns_server_destroy(None) == 1
+    assert lib.sns_server_step(None, None, 0, None, None, None, None) == 1
+    assert lib.sns_server_submit(None, None, None) == 1
+
+
+def test_batch_and_server_reject_bad_arguments(lib):
+    from spectral_solver_b200 import _lib
+    b = C.c_void_p()
+    assert lib.sns_batch_create(None, 0, 0, None, C.byref(b), None) == 1
+    assert not b.value
+    s = C.c_void_p()
+    assert lib.sns_server_create(0, 1, C.byref(s)) == 1  # zero budget
+    assert lib.sns_server_create(1 << 30, 7, C.byref(s)) == 1  # unknown precision
+    assert not s.value
+    assert len(lib.sns_last_error(None)) > 0
 
 
 @pytest.mark.skipif(has_gpu(), reason="checks the no-device path")

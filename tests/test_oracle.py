@@ -105,3 +105,23 @@ def test_oracle_golden_64_adaptive_t20():
     assert rel(last["enstrophy"], 0.98804555508950165) < 1e-11
     assert rel(last["max_velocity"], 0.48555765715015353) < 1e-10
     assert last["max_spectral_divergence"] < 1e-11
+
+
+def test_integrating_factor_oracle_limits():
+    """The oracle's integrating-factor RK3: with nu = 0 the factor is 1 and the explicit
+    scheme's viscous term is 0, so the two agree bit for bit; with nu > 0 they differ by the
+    schemes' truncation error only (dt = 1e-2, 10 steps at 12^3, nu = 0.05)."""
+    import numpy as np
+    from oracle.ref_r2c import TaylorGreenR2C
+    for nu, tol in ((0.0, 0.0), (0.05, 1e-6)):
+        a = TaylorGreenR2C(12, 1.0, workers=1)
+        b = TaylorGreenR2C(12, 1.0, workers=1, integrating_factor=True)
+        a.nu = b.nu = nu
+        for _ in range(10):
+            a.step(1e-2)
+            b.step(1e-2)
+        num = sum(float(np.sum(np.abs(x - y) ** 2)) for x, y in zip(a.u_hat, b.u_hat))
+        den = sum(float(np.sum(np.abs(y) ** 2)) for y in a.u_hat)
+        assert (num / den) ** 0.5 <= tol
+        if nu > 0:
+            assert num > 0.0
