@@ -117,6 +117,14 @@ int sns_dump_velocity(sns_handle* h, double* const phys[3]);
  * own viscosity to the backend's handle). */
 int sns_set_viscosity(sns_handle* h, double nu);
 
+/* Nonlinear term: the reference's conservative form -i k_j FFT(u_i u_j) (default), or the
+ * rotational form FFT(u x omega), omega_hat = i k x u_hat, with the same phase-shift
+ * dealiasing, sphere mask and projection.  The two differ by a gradient (removed by the
+ * projection) and by their aliasing residue, so the rotational form is not a parity mode.
+ * It needs 3 more device fields (allocated by the first switch to it). */
+enum { SNS_FORM_CONSERVATIVE = 0, SNS_FORM_ROTATIONAL = 1 };
+int sns_set_nonlinear_form(sns_handle* h, int form);
+
 /* Persistent grids chosen at creation: out[0] TMA y/z passes, out[1] two-stage x pass
  * (0 = generic), out[2] fused forward-z + sweep (0 = two kernels), out[3] SM count. */
 int sns_launch_config(const sns_handle* h, int* out, int count);

@@ -62,7 +62,7 @@ class TaylorGreenR2C:
     """Half-spectrum restatement of ``TaylorGreenSolver::Impl`` with identical numerics."""
 
     def __init__(self, n: int, reynolds: float, u_hat0=None, workers: int | None = None,
-                 integrating_factor: bool = False):
+                 integrating_factor: bool = False, rotational: bool = False):
         if n <= 0:
             raise ValueError("grid size must be positive")
         if reynolds <= 0.0:
@@ -70,6 +70,7 @@ class TaylorGreenR2C:
         self.n = n
         self.nu = 1.0 / reynolds
         self.integrating_factor = integrating_factor
+        self.rotational = rotational
         self.global_size = n * n * n
         self.workers = WORKERS if workers is None else workers
         mx, my, mz = half_mode_grids(n)
@@ -133,10 +134,31 @@ class TaylorGreenR2C:
                 rhs[b] = rhs[b] + (-1j) * kv[a] * value
         return rhs
 
+    def nonlinear_rotational(self, u_hat):
+        """Rotational-form nonlinear term u x omega, omega_hat = i k x u_hat, with the same
+        phase-shift dealiasing and sphere mask as the conservative form.  The two forms
+        differ by a gradient (removed by the projection) and by their aliasing residue.
+        The reference implements only the conservative form; this is the project's own
+        specification of the alternative (SURVEY.md's next-step list names it)."""
+        kx, ky, kz = self.kvals
+        w_hat = [1j * (ky * u_hat[2] - kz * u_hat[1]), 1j * (kz * u_hat[0] - kx * u_hat[2]),
+                 1j * (kx * u_hat[1] - ky * u_hat[0])]
+        u0 = [self.backward_real(u) for u in u_hat]
+        w0 = [self.backward_real(w) for w in w_hat]
+        us = [self.backward_real(u * self.phase) for u in u_hat]
+        ws = [self.backward_real(w * self.phase) for w in w_hat]
+
+        def cross(a, b):
+            return [a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2], a[0] * b[1] - a[1] * b[0]]
+
+        c0, cs = cross(u0, w0), cross(us, ws)
+        cphase = np.conj(self.phase)
+        return [np.where(self.keep, 0.5 * (self.forward(a) + self.forward(b) * cphase), 0.0) for a, b in zip(c0, cs)]
+
     def compute_rhs(self, u_hat=None):
         if u_hat is None:
             u_hat = self.u_hat
-        rhs = self.nonlinear(u_hat)
+        rhs = self.nonlinear_rotational(u_hat) if self.rotational else self.nonlinear(u_hat)
         if not self.integrating_factor:
             for c in range(3):
                 rhs[c] = rhs[c] - u_hat[c] * (self.nu * self.k2)

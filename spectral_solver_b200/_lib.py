@@ -72,6 +72,7 @@ SIGNATURES = {
     "sns_max_velocity": (C.c_int, [_H, _DP]),
     "sns_dump_velocity": (C.c_int, [_H, _DPP]),
     "sns_set_viscosity": (C.c_int, [_H, C.c_double]),
+    "sns_set_nonlinear_form": (C.c_int, [_H, C.c_int]),
     "sns_launch_config": (C.c_int, [_H, C.POINTER(C.c_int), C.c_int]),
     "sns_grid_size": (C.c_int, [_H]),
     "sns_device_bytes": (C.c_size_t, [_H]),
@@ -251,6 +252,10 @@ class Solver:
         out = (C.c_int * 4)()
         self._check(self.lib.sns_launch_config(self.h, out, 4))
         return dict(tma_grid=out[0], xpass_grid=out[1], p5_grid=out[2], sms=out[3])
+
+    def set_nonlinear_form(self, form: int):
+        """0: the reference's conservative form (default), 1: the rotational form u x omega."""
+        self._check(self.lib.sns_set_nonlinear_form(self.h, form))
 
     def device_bytes(self) -> int:
         return int(self.lib.sns_device_bytes(self.h))

@@ -93,6 +93,9 @@ struct sns_handle {
   CUtensorMap map_state_z{};  // state fields (u[3], g[3]), z-pencil boxes
   CUtensorMap map_work_y{};   // 12 work fields, y-pencil boxes
   CUtensorMap map_work_z{};   // 12 work fields, z-pencil boxes
+  int form = 0;               // nonlinear form: 0 conservative (the reference), 1 rotational
+  char* xf = nullptr;         // rotational form: omega_hat (3 fields), allocated on first use
+  CUtensorMap map_x_z{};      // the omega_hat fields, z-pencil boxes
   size_t partial_count = 0;
   size_t bytes = 0;
   int fail_after = 0;
@@ -297,9 +300,69 @@ inline void mark(PassMarks* pm, int i, cudaStream_t st) {
   if (pm && pm->on) cudaEventRecord(pm->ev[i], st);
 }
 
+sns::SweepArgs stage_args(const sns_handle* h, int stage, double dt, int mode) {
+  sns::SweepArgs a{};
+  a.nu = h->nu;
+  a.stage = stage;
+  a.mode = mode;
+  a.dealias = 1;
+  // integrating-factor mode: after stage s, u and g advance from c_s*dt to c_{s+1}*dt with
+  // the stage times c = (0, 1/3, 3/4, 1) of the Williamson scheme
+  a.visc_if = h->viscous_mode == SNS_VISCOUS_INTEGRATING_FACTOR ? 1 : 0;
+  a.if_tau = stage == 0 ? dt / 3.0 : (stage == 1 ? 5.0 * dt / 12.0 : dt / 4.0);
+  if (stage == 0) {
+    a.ga = 0.0;
+    a.ub = dt / 3.0;
+  } else if (stage == 1) {
+    a.ga = -5.0 / 9.0;
+    a.ub = 15.0 * dt / 16.0;
+  } else {
+    a.ga = -153.0 / 128.0;
+    a.ub = 8.0 * dt / 15.0;
+  }
+  return a;
+}
+
+// One stage in the rotational form: omega_hat, inverse z (+ phase) of u and omega, inverse y
+// of the 12 fields, the u x omega x pass, forward y and z of the 6 products, the sweep.
+void run_stage_rot(sns_handle* h, char* u_src, char* g_buf, int stage, double dt, int mode, char* rhs_out,
+                   PassMarks* pm) {
+  const sns::Ops* o = h->ops;
+  const sns::Geom& g = h->g;
+  cudaStream_t st = h->stream;
+  const int tiles_in = h->nyq_clean ? h->tiles_data() : h->tiles_all();
+  const int f_src = (int)((size_t)(u_src - h->state) / h->fbytes);
+  mark(pm, 0, st);
+  o->omega_hat(u_src, h->xf, g, st);
+  o->yz_tma(h->map_state_z, 2, +1, 1, tma_args(h, f_src, 3, tiles_in, h->work, 0, h->inv_size()), h->tw, h->phase, g,
+            h->tma_grid, st);
+  o->yz_tma(h->map_x_z, 2, +1, 1, tma_args(h, 0, 3, tiles_in, h->work, 6, h->inv_size()), h->tw, h->phase, g,
+            h->tma_grid, st);
+  mark(pm, 1, st);
+  o->yz_tma(h->map_work_y, 1, +1, 0, tma_args(h, 0, 12, tiles_in, h->work, 0, 1.0), h->tw, h->phase, g, h->tma_grid,
+            st);
+  mark(pm, 2, st);
+  o->xpass_rot(h->work, u_src, h->xf, h->phase, h->inv_size(), h->nyq_clean ? 1 : 0, h->tw, g, st);
+  mark(pm, 3, st);
+  o->nyq_reduce(h->work, h->nyq_part, g, st);  // the first 6 sums are the products'
+  mark(pm, 4, st);
+  o->yz_tma(h->map_work_y, 1, -1, 0, tma_args(h, 0, 6, h->tiles_data(), h->work, 0, 1.0), h->tw, h->phase, g,
+            h->tma_grid, st);
+  mark(pm, 5, st);
+  o->yz_tma(h->map_work_z, 2, -1, 0, tma_args(h, 0, 6, h->tiles_data(), h->work, 0, 1.0), h->tw, h->phase, g,
+            h->tma_grid, st);
+  mark(pm, 6, st);
+  o->sweep_rot(h->work, u_src, g_buf, rhs_out, h->nyq_part, h->phase, stage_args(h, stage, dt, mode), g, st);
+  mark(pm, 7, st);
+}
+
 // One RK3 stage (or the RHS only, mode 1) on u_src: the five fused passes.
 void run_stage(sns_handle* h, char* u_src, char* g_buf, int stage, double dt, int mode, char* rhs_out,
                double* partials, PassMarks* pm = nullptr) {
+  if (h->form == 1) {
+    run_stage_rot(h, u_src, g_buf, stage, dt, mode, rhs_out, pm);
+    return;
+  }
   const sns::Ops* o = h->ops;
   const sns::Geom& g = h->g;
   cudaStream_t st = h->stream;
@@ -332,25 +395,7 @@ void run_stage(sns_handle* h, char* u_src, char* g_buf, int stage, double dt, in
     o->yz_tma(h->map_work_z, 2, -1, 0, tma_args(h, 0, 12, h->tiles_data(), h->work, 0, 1.0), h->tw, h->phase, g,
               h->tma_grid, st);
   mark(pm, 6, st);
-  sns::SweepArgs a{};
-  a.nu = h->nu;
-  a.stage = stage;
-  a.mode = mode;
-  a.dealias = 1;
-  // integrating-factor mode: after stage s, u and g advance from c_s*dt to c_{s+1}*dt with
-  // the stage times c = (0, 1/3, 3/4, 1) of the Williamson scheme
-  a.visc_if = h->viscous_mode == SNS_VISCOUS_INTEGRATING_FACTOR ? 1 : 0;
-  a.if_tau = stage == 0 ? dt / 3.0 : (stage == 1 ? 5.0 * dt / 12.0 : dt / 4.0);
-  if (stage == 0) {
-    a.ga = 0.0;
-    a.ub = dt / 3.0;
-  } else if (stage == 1) {
-    a.ga = -5.0 / 9.0;
-    a.ub = 15.0 * dt / 16.0;
-  } else {
-    a.ga = -153.0 / 128.0;
-    a.ub = 8.0 * dt / 15.0;
-  }
+  const sns::SweepArgs a = stage_args(h, stage, dt, mode);
   if (fused)
     o->p5(h->map_work_z, u_src, g_buf, rhs_out, h->nyq_part, nparts, h->tw, h->phase, a, h->tiles_data(), g,
           h->p5_grid, h->err_word, st);
@@ -444,6 +489,7 @@ void release(sns_handle* h) {
   cudaFree(h->err_word);
   cudaFree(h->tw2);
   cudaFree(h->nyq_part);
+  cudaFree(h->xf);
   if (h->ev0) cudaEventDestroy(h->ev0);
   if (h->ev1) cudaEventDestroy(h->ev1);
   if (h->stream) cudaStreamDestroy(h->stream);
@@ -656,6 +702,29 @@ int sns_set_viscosity(sns_handle* h, double nu) {
   }
   h->nu = nu;
   return SNS_OK;
+}
+
+int sns_set_nonlinear_form(sns_handle* h, int form) {
+  return guarded(h, [&] {
+    if (form != SNS_FORM_CONSERVATIVE && form != SNS_FORM_ROTATIONAL)
+      throw SnsError(SNS_ERR_INVALID, "form must be SNS_FORM_CONSERVATIVE (0) or SNS_FORM_ROTATIONAL (1)");
+    if (form == SNS_FORM_ROTATIONAL && h->xf == nullptr) {
+      size_t free_b = 0, total_b = 0;
+      ck(cudaMemGetInfo(&free_b, &total_b), "cudaMemGetInfo");
+      if (3 * h->fbytes > free_b) throw SnsError(SNS_ERR_NOMEM, "no room for the 3 vorticity fields");
+      const cudaError_t e = cudaMalloc((void**)&h->xf, 3 * h->fbytes);
+      if (e != cudaSuccess) {
+        cudaGetLastError();
+        h->xf = nullptr;
+        throw SnsError(SNS_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+      }
+      h->bytes += 3 * h->fbytes;
+      ck(cudaMemsetAsync(h->xf, 0, 3 * h->fbytes, h->stream), "memset");  // padding columns stay zero
+      h->map_x_z = make_field_map(h->xf, 3, 2, h->g, h->cbytes);
+      sync(h, "sns_set_nonlinear_form");
+    }
+    h->form = form;
+  });
 }
 
 int sns_launch_config(const sns_handle* h, int* out, int count) {

@@ -975,6 +975,164 @@ __global__ void __launch_bounds__(32) k_nyq_mode(C* __restrict__ u, C* __restric
 }
 
 // ------------------------------------------------------------------------------------
+// Rotational form (selectable; the reference computes only the conservative form).
+// omega_hat = i k x u_hat on every stored mode (the wavenumbers of the stored modes, index
+// N/2 -> +N/2, as the conservative form's -i k uses them).
+template <class C>
+__global__ void k_omega_hat(const C* __restrict__ u, C* __restrict__ w, Geom g) {
+  const long long total = (long long)g.n * g.n * (g.nh + 1);
+  const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= total) return;
+  using RT = real_of<C>;
+  const long long row = e / (g.nh + 1);
+  const int ix = (int)(e % (g.nh + 1));
+  const RT kx = (RT)ix, ky = (RT)signed_mode((int)(row % g.n), g.n), kz = (RT)signed_mode((int)(row / g.n), g.n);
+  const long long idx = row * g.pitch + ix;
+  const C u0 = u[idx], u1 = u[g.field + idx], u2 = u[2 * g.field + idx];
+  // i * (a) = (-a.y, a.x)
+  auto i_times = [](RT ax, RT ay) { return cmk(-ay, ax); };
+  w[idx] = i_times(ky * u2.x - kz * u1.x, ky * u2.y - kz * u1.y);
+  w[g.field + idx] = i_times(kz * u0.x - kx * u2.x, kz * u0.y - kx * u2.y);
+  w[2 * g.field + idx] = i_times(kx * u1.x - ky * u0.x, kx * u1.y - ky * u0.y);
+}
+
+// Rotational x pass, one row (y, z) per CTA.  Inputs after the inverse y/z passes: work
+// fields 2c, 2c+1 = U_c, V_c (velocity on both grids), 6 + 2c, 7 + 2c = Omega_c, Psi_c
+// (vorticity on both grids).  Inverse x of the 6 packed pairs, u x omega on both grids,
+// forward x of the 3 packed components; outputs: work fields 2c, 2c+1 = A_c, B_c.
+template <int N, class C>
+__global__ void __launch_bounds__(nt_x<N>())
+k_xpass_rot(C* __restrict__ work, const C* __restrict__ unyq, const C* __restrict__ wnyq,
+            const C* __restrict__ phase, double scale, int nyq_scalar, const C* __restrict__ tw, Geom g) {
+  constexpr int NT = nt_x<N>();
+  constexpr int NH = N / 2;
+  constexpr int RP = row_pitch(N);
+  extern __shared__ __align__(16) unsigned char smraw_x[];
+  C* smem = reinterpret_cast<C*>(smraw_x);
+  C* s_tw = smem;
+  C* seq = smem + N;  // 6 sequences of pitch RP
+  const int tid = threadIdx.x;
+  load_twiddles<N>(s_tw, tw, tid, NT);
+  const long long rbase = (long long)blockIdx.x * g.pitch;
+  for (int e = tid; e < 6 * (NH + 1); e += NT) {
+    const int q = e / (NH + 1), k = e % (NH + 1);
+    const int c = q % 3, vort = q / 3;
+    C A, B;
+    if (k == NH && nyq_scalar) {
+      // masked state: the plane mx = N/2 holds only (N/2,0,0), a constant after the y/z
+      // inverse transforms (times the phase on the shifted grid)
+      const C cn = cscale((vort ? wnyq : unyq)[(long long)c * g.field + NH], scale);
+      A = cn;
+      B = cmul(cn, phase[NH + 3 * N / 2]);
+    } else {
+      A = work[(long long)(6 * vort + 2 * c) * g.field + rbase + k];
+      B = work[(long long)(6 * vort + 2 * c + 1) * g.field + rbase + k];
+    }
+    C zk, zm;
+    pack_pair(A, B, k, NH, N, &zk, &zm);
+    C* sq = seq + q * RP;
+    sq[k + (k >> 3)] = zk;
+    if (k != 0 && k != NH) sq[(N - k) + ((N - k) >> 3)] = zm;
+  }
+  __syncthreads();
+  smem_fft<N, +1, 6, NT, RowTile<RP>>(seq, s_tw, tid);
+  for (int x = tid; x < N; x += NT) {
+    const int p = x + (x >> 3);
+    C uu[3], ww[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      uu[c] = seq[c * RP + p];        // (u_c, u_c shifted)
+      ww[c] = seq[(3 + c) * RP + p];  // (omega_c, omega_c shifted)
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const int a = (c + 1) % 3, b = (c + 2) % 3;
+      seq[c * RP + p] = cmk(uu[a].x * ww[b].x - uu[b].x * ww[a].x, uu[a].y * ww[b].y - uu[b].y * ww[a].y);
+    }
+  }
+  __syncthreads();
+  smem_fft<N, -1, 3, NT, RowTile<RP>>(seq, s_tw, tid);
+  for (int e = tid; e < 3 * (NH + 1); e += NT) {
+    const int c = e / (NH + 1), k = e % (NH + 1);
+    const int km = (N - k) % N;
+    C A, B;
+    unpack_pair(seq[c * RP + k + (k >> 3)], seq[c * RP + km + (km >> 3)], &A, &B);
+    work[(long long)(2 * c) * g.field + rbase + k] = A;
+    work[(long long)(2 * c + 1) * g.field + rbase + k] = B;
+  }
+}
+
+// Rotational k-space sweep: r_c = the dealiased, masked (u x omega)_c (no -i k), then the
+// shared viscous / integrating-factor, Leray projection and RK3 update of finish_mode.
+// The (N/2,0,0) mode takes its two-grid values from the plane sums of the 6 product fields.
+template <int N, class C>
+__global__ void __launch_bounds__(256)
+k_sweep_rot(const C* __restrict__ work, C* __restrict__ u, C* __restrict__ gbuf, C* __restrict__ rhs,
+            const double* __restrict__ nyq_sums, const C* __restrict__ phase, SweepArgs a, Geom g) {
+  constexpr int NH = N / 2;
+  const long long e = (long long)blockIdx.x * 256 + threadIdx.x;
+  const long long total = (long long)N * N * NH;
+  const bool load_g = a.stage > 0;
+  using RT = real_of<C>;
+  auto update = [&](long long idx, int mx, int my, int mz, const C* A, const C* B, C ph) {
+    const int m2 = mx * mx + my * my + mz * mz;
+    const bool keep = 4LL * m2 <= (long long)N * N;
+    C r[3], uu[3], gg[3], rr[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      r[c] = pair_value(A[c], B[c], ph, keep, a.dealias);
+      uu[c] = u[(long long)c * g.field + idx];
+      gg[c] = load_g ? gbuf[(long long)c * g.field + idx] : czero<C>();
+    }
+    finish_mode(r, mx, my, mz, N, uu, gg, load_g, rr, a);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      if (a.mode != 0) {
+        rhs[(long long)c * g.field + idx] = rr[c];
+      } else {
+        u[(long long)c * g.field + idx] = uu[c];
+        gbuf[(long long)c * g.field + idx] = gg[c];
+      }
+    }
+  };
+  if (e < total) {
+    const long long row = e / NH;
+    const int mx = (int)(e % NH);
+    const int my = signed_mode((int)(row % N), N);
+    const int mz = signed_mode((int)(row / N), N);
+    const long long idx = row * g.pitch + mx;
+    C A[3], B[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      A[c] = work[(long long)(2 * c) * g.field + idx];
+      B[c] = work[(long long)(2 * c + 1) * g.field + idx];
+    }
+    update(idx, mx, my, mz, A, B, phase[mx + my + mz + 3 * N / 2]);
+    if (mx == 0 && row != 0) {  // the plane mx = N/2 is zero off (N/2,0,0) after the mask
+      const long long inq = row * g.pitch + NH;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        if (a.mode != 0) {
+          rhs[(long long)c * g.field + inq] = czero<C>();
+        } else {
+          u[(long long)c * g.field + inq] = czero<C>();
+          gbuf[(long long)c * g.field + inq] = czero<C>();
+        }
+      }
+    }
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    C A[3], B[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      A[c] = cmk((RT)nyq_sums[2 * c], RT(0));
+      B[c] = cmk((RT)nyq_sums[2 * c + 1], RT(0));
+    }
+    update(NH, NH, 0, 0, A, B, phase[NH + 3 * N / 2]);
+  }
+}
+
+// ------------------------------------------------------------------------------------
 // P5 fused (N = 128, 256, 512): forward z pass of the 12 product fields and the whole
 // k-space sweep in one persistent kernel, so the transformed products never return to HBM.
 // A tile is (TW columns mx, one my, all mz); its 12 field tiles arrive one after another
@@ -1608,6 +1766,21 @@ struct Launch {
       return 0;
     }
   }
+  static void omega_hat(const void* u, void* w, Geom g, cudaStream_t st) {
+    const long long total = (long long)N * N * (N / 2 + 1);
+    k_omega_hat<C><<<(unsigned)((total + 255) / 256), 256, 0, st>>>(F(u), F(w), g);
+  }
+  static void xpass_rot(void* work, const void* unyq, const void* wnyq, const void* phase, double scale,
+                        int nyq_scalar, const void* tw, Geom g, cudaStream_t st) {
+    k_xpass_rot<N, C><<<N * N, nt_x<N>(), x_smem(6), st>>>(F(work), F(unyq), F(wnyq), F(phase), scale, nyq_scalar,
+                                                           F(tw), g);
+  }
+  static void sweep_rot(const void* work, void* u, void* gbuf, void* rhs, const double* nyq_sums, const void* phase,
+                        SweepArgs a, Geom g, cudaStream_t st) {
+    const long long total = (long long)N * N * (N / 2);
+    k_sweep_rot<N, C><<<(unsigned)((total + 255) / 256), 256, 0, st>>>(F(work), F(u), F(gbuf), F(rhs), nyq_sums,
+                                                                       F(phase), a, g);
+  }
   static void xpass_r2c(const double* in, void* out, int nf, const void* tw, Geom g, cudaStream_t st) {
     k_xpass_r2c<N, C><<<dim3(N * N / 2, nf), nt_x<N>(), x_smem(1), st>>>(in, F(out), F(tw), g);
   }
@@ -1664,11 +1837,12 @@ struct Launch {
     set_smem(k_xpass_r2c<N, C>, x_smem(1));
     set_smem(k_xpass_c2r<N, C>, x_smem(1));
     set_smem(k_xpass_diag<N, C>, x_smem(2));
+    set_smem(k_xpass_rot<N, C>, x_smem(6));
   }
   static const Ops* table() {
     static const Ops ops = {N,  (int)sizeof(C), kT, init, zpass_inv_phase, ypass, zpass, xpass_products, nyq_reduce,
                             sweep, xpass_r2c, xpass_c2r, xpass_diag, yz_tma, tma_blocks_per_sm, xpass2, xpass2_grid,
-                            p5, p5_grid};
+                            p5, p5_grid, omega_hat, xpass_rot, sweep_rot};
     return &ops;
   }
 };

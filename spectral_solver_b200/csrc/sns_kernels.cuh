@@ -94,6 +94,13 @@ struct Ops {
   void (*p5)(const CUtensorMap& map, void* u, void* gbuf, void* rhs, const double* nyq_part, int nparts,
              const void* tw, const void* phase, SweepArgs a, int ncb, Geom g, int grid, int* err, cudaStream_t st);
   int (*p5_grid)(int nsm);
+  // rotational form: omega_hat = i k x u_hat (3 fields); the x pass forming u x omega on both
+  // grids (12 inputs -> 6 outputs in work fields 0..5); the sweep combining the two grids
+  void (*omega_hat)(const void* u, void* w, Geom g, cudaStream_t st);
+  void (*xpass_rot)(void* work, const void* unyq, const void* wnyq, const void* phase, double scale, int nyq_scalar,
+                    const void* tw, Geom g, cudaStream_t st);
+  void (*sweep_rot)(const void* work, void* u, void* gbuf, void* rhs, const double* nyq_sums, const void* phase,
+                    SweepArgs a, Geom g, cudaStream_t st);
 };
 
 // nullptr when the size has no FFT plan; precision 0 = FP64, 1 = FP32
