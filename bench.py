@@ -184,6 +184,31 @@ def cpu_oracle_rate(n: int, sample_stages: int = 1):
     return n ** 3 * steps / dt / 1e9, dt, threads
 
 
+def cpu_model() -> str:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def cpu_oracle_config1(steps: int = 40):
+    """The CPU oracle on configuration 1's grid (64^3 FP64, dt 5e-3): `steps` RK3 steps, for
+    comparison with the reference's published single-rank FFTW rates at 64^3."""
+    from oracle import ref_r2c
+    threads = os.cpu_count() or 1
+    s = ref_r2c.TaylorGreenR2C(64, RE, workers=threads)
+    s.step(5e-3)  # plans and caches
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        s.step(5e-3)
+    dt = time.perf_counter() - t0
+    return 64 ** 3 * steps / dt, dt, threads
+
+
 def run_reference(args, world, rank, pg):
     """--impl reference: the reference's CPU path on the host cores.  The reference itself
     cannot be built here (FFTW3, MPI, AVA and FLUPS are absent), so its CPU restatement
@@ -312,9 +337,14 @@ def run_b200(args, world, rank, local, pg):
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
             rate, secs, threads = cpu_oracle_rate(n, 1)
+            r64, s64, _ = cpu_oracle_config1()
             cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
                    "sample": f"1 RK3 stage at {n}^3 ({secs:.1f} s) of the CPU oracle (oracle/ref_r2c.py, scipy "
-                             f"pocketfft, {threads} threads, FP64); the reference's FFTW path cannot be built here"}
+                             f"pocketfft, {threads} threads, FP64); the reference's FFTW path cannot be built here",
+                   "cpu_model": cpu_model(),
+                   "config1_64": {"value": r64 / 1e9, "unit": UNIT, "gpt_steps_per_s": r64,
+                                  "sample": f"40 RK3 steps at 64^3, dt 5e-3 ({s64:.1f} s, {threads} threads)",
+                                  "reference_published_gpt_steps_per_s": [1.39e6, 2.47e6]}}
         r = results[head]
         cb = 16 if head == "fp64" else 8
         resident = 18 * n * n * (((n // 2 + 1) + 128 // cb - 1) // (128 // cb) * (128 // cb)) * cb / 1e9
