@@ -26,3 +26,11 @@ def lib():
     """The C-ABI library, loaded through the package's ctypes binding."""
     from spectral_solver_b200 import _lib
     return _lib.load()
+
+
+def golden_finals() -> dict:
+    """The reference's published FP64 t = 20 finals (tests/golden/benchmark_finals.json,
+    extracted from its Benchmark.md by tests/golden/make_golden.py), keyed by N."""
+    import json
+    with open(os.path.join(ROOT, "tests", "golden", "benchmark_finals.json")) as f:
+        return {r["n"]: r for r in json.load(f)["runs"]}

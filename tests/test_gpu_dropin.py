@@ -64,17 +64,11 @@ def test_config1_cli_matches_oracle(tmp_path):
     assert max(float(np.max(np.abs(vel[c] - ref_vel[c]))) for c in range(3)) < 1e-10
 
 
-GOLDEN = {
-    # n: (steps, E, eps, max_u) -- FP64 finals at t = 20 published by the reference
-    64: (352, 0.016877965072920623, 0.0012350569438618771, 0.48555765715015353),   # Benchmark.md:644-649
-    128: (740, 0.021553419004393556, 0.0019026009263740915, 0.54486119854790893),  # Benchmark.md:749-754
-    256: (1527, 0.021598156223318035, 0.0019036857700047299, 0.52982227104531054),  # Benchmark.md:777-782
-}
-
-
 @pytest.mark.parametrize("n", [64, 128, 256])
 def test_golden_t20_through_cli(tmp_path, n):
-    steps, e, eps, umax = GOLDEN[n]
+    from tests.conftest import golden_finals
+    g = golden_finals()[n]  # the reference's published FP64 finals (tests/golden/)
+    steps, e, eps, umax = g["steps"], g["kinetic_energy"], g["dissipation"], g["max_velocity"]
     rows, out = run_cli(["--n", str(n), "--re", "1600", "--adaptive-cfl", "1", "--dt", "0.5", "--cfl", "0.5",
                          "--t-end", "20", "--output-dt", "1", "--print-every", "20"], tmp_path, timeout=1800)
     assert len(rows) == 21

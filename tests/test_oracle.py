@@ -100,10 +100,13 @@ def test_oracle_golden_64_adaptive_t20():
     assert steps == 352
     assert len(rows) == 21
     last = rows[-1]
-    assert rel(last["kinetic_energy"], 0.016877965072920623) < 1e-11
-    assert rel(last["dissipation"], 0.0012350569438618771) < 1e-11
-    assert rel(last["enstrophy"], 0.98804555508950165) < 1e-11
-    assert rel(last["max_velocity"], 0.48555765715015353) < 1e-10
+    from tests.conftest import golden_finals
+    g = golden_finals()[64]  # Benchmark.md:281, 647-648 via tests/golden/benchmark_finals.json
+    assert steps == g["steps"]
+    assert rel(last["kinetic_energy"], g["kinetic_energy"]) < 1e-11
+    assert rel(last["dissipation"], g["dissipation"]) < 1e-11
+    assert rel(last["enstrophy"], g["enstrophy"]) < 1e-11
+    assert rel(last["max_velocity"], g["max_velocity"]) < 1e-10
     assert last["max_spectral_divergence"] < 1e-11
 
 
@@ -125,3 +128,15 @@ def test_integrating_factor_oracle_limits():
         assert (num / den) ** 0.5 <= tol
         if nu > 0:
             assert num > 0.0
+
+
+def test_golden_fixture_is_the_published_record():
+    """tests/golden/benchmark_finals.json holds the three FP64 runs the parity tests pin
+    (64^3 FFTW, 128^3 and 256^3 cuFFT), with the step counts of the same runs."""
+    from tests.conftest import golden_finals
+    g = golden_finals()
+    assert sorted(g) == [64, 128, 256]
+    assert [g[n]["steps"] for n in (64, 128, 256)] == [352, 740, 1527]
+    assert g[64]["kinetic_energy"] == 0.016877965072920623 and g[256]["dissipation"] == 0.0019036857700047299
+    for r in g.values():
+        assert all(v.startswith("Benchmark.md:") for v in r["source"].values())
