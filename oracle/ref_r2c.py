@@ -139,7 +139,7 @@ class TaylorGreenR2C:
         phase-shift dealiasing and sphere mask as the conservative form.  The two forms
         differ by a gradient (removed by the projection) and by their aliasing residue.
         The reference implements only the conservative form; this is the project's own
-        specification of the alternative (SURVEY.md's next-step list names it)."""
+        specification of the alternative."""
         kx, ky, kz = self.kvals
         w_hat = [1j * (ky * u_hat[2] - kz * u_hat[1]), 1j * (kz * u_hat[0] - kx * u_hat[2]),
                  1j * (kx * u_hat[1] - ky * u_hat[0])]
