@@ -418,11 +418,15 @@ k_xpass_products(C* __restrict__ work, const C* __restrict__ unyq, const C* __re
 //   inverse stage A : radix 16 over stride-M inputs, the packing Z = U + iV (with the
 //                     mirror and the real-part rule at mx = 0, N/2) fused into the loads
 //   inverse stage B : radix M (M = 32 split over lane pairs, combined by a shuffle);
-//                     z_c = u_c + i*u_shifted_c lands in the (consumed) staging buffer
+//                     z_c = u_c + i*u_shifted_c lands in work region 3 + c
 //   forward stage A : the products p0 + i*ps fused into the loads, radix 16
 //   forward stage B : radix M, then the r2c unpack P0(k), Ps(k) = (Z(k) +- conj Z(N-k))/2
 //                     with the mirror fetched from the partner lane by a shuffle, and
 //                     128-byte stores straight to HBM
+// Both stages of one FFT run on the same warp (half-warp for N = 256), so they meet at a
+// __syncwarp; the CTA synchronises twice per row group: before it starts (the previous
+// group is done, its staging buffer is refilled) and between the inverse and forward
+// FFTs (each product reads two components).
 // The (N/2,0,0) sums of the 12 product planes accumulate in registers per CTA.
 template <int N, class C>
 struct XP {
@@ -494,10 +498,7 @@ k_xpass2(C* __restrict__ work, const C* __restrict__ unyq, const C* __restrict__
                   X::kRowBytes, &bars[b]);
     }
   };
-  if (tid == 0) {
-    if (blockIdx.x < niter) issue(blockIdx.x, 0);
-    if (blockIdx.x + gridDim.x < niter) issue(blockIdx.x + gridDim.x, 1);
-  }
+  if (tid == 0 && blockIdx.x < niter) issue(blockIdx.x, 0);
   double nyq_p0 = 0.0, nyq_ps = 0.0;  // owned by the lane that holds k = N/2 of its pair
   int k = 0;
   for (long long it = blockIdx.x; it < niter; ++k, it += gridDim.x) {
@@ -505,14 +506,13 @@ k_xpass2(C* __restrict__ work, const C* __restrict__ unyq, const C* __restrict__
     const uint32_t parity = (uint32_t)(k >> 1) & 1u;
     if (tid == 0 && !mbar_wait_bounded(&bars[b], parity)) s_fail = 1;
     __syncthreads();
-    if (s_fail) {
-      if (tid == 0) {
-        atomicExch(err, kErrTmaTimeout);
-        (void)mbar_wait_bounded(&bars[b ^ 1], (uint32_t)((k + 1) >> 1) & 1u);
-      }
+    if (s_fail) {  // no other copy is in flight: the next row is issued after this wait
+      if (tid == 0) atomicExch(err, kErrTmaTimeout);
       return;
     }
     (void)mbar_try_wait(&bars[b], parity);
+    // every thread has finished the previous row, so its staging buffer takes the next one
+    if (tid == 0 && it + gridDim.x < niter) issue(it + gridDim.x, b ^ 1);
     C* S = stg + b * ROWS * STG;
 
     // ---- inverse stage A: (r, c, t), packing fused into the loads
@@ -551,9 +551,9 @@ k_xpass2(C* __restrict__ work, const C* __restrict__ unyq, const C* __restrict__
 #pragma unroll
       for (int q = 0; q < 16; ++q) Wc[pp16(16 * t + q)] = v[q];
     }
-    __syncthreads();
+    __syncwarp();
 
-    // ---- inverse stage B: z_c into the staging buffer (its inputs are consumed)
+    // ---- inverse stage B: z_c into work region 3 + c
     if constexpr (X::PAIR) {
       if (tid < ROWS * 96) {
         const int lane = tid & 31, c = (tid >> 5) % 3, r = tid / 96, j = lane & 15, h = lane >> 4;
@@ -569,7 +569,7 @@ k_xpass2(C* __restrict__ work, const C* __restrict__ unyq, const C* __restrict__
 #pragma unroll
           for (int q = 1; q < 16; ++q) v[q] = cmulc(v[q], tw2[16 * 16 + q]);  // conj W32^q
         }
-        C* Zc = S + r * STG + c * SP;
+        C* Zc = W + (r * 6 + 3 + c) * SP;
 #pragma unroll
         for (int q = 0; q < 16; ++q) {
           const C o = shfl2_xor(v[q], 16);
@@ -585,111 +585,117 @@ k_xpass2(C* __restrict__ work, const C* __restrict__ unyq, const C* __restrict__
 #pragma unroll
         for (int q = 0; q < 16; ++q) v[q] = q == 0 ? Wc[pp16(j)] : cmulc(Wc[pp16(j + 16 * q)], tw2[q * 16 + j]);
         dft16<+1>(v);
-        C* Zc = S + r * STG + c * SP;
+        C* Zc = W + (r * 6 + 3 + c) * SP;
 #pragma unroll
         for (int q = 0; q < 16; ++q) Zc[pp16(j + 16 * q)] = v[q];
       }
     }
     __syncthreads();
 
-    // ---- forward stage A: products fused into the loads
+    // ---- forward stages, per row group; the warp (half-warp for N = 256) of product ab
+    // runs both stages of its FFT.  Product ab lands in work region ab (ab < 3, free since
+    // the inverse stage B) or in the consumed staging rows (ab >= 3).
     constexpr int FWD_ROWS = X::NT / (6 * M);  // rows one pass of the CTA covers
+    static_assert(X::PAIR ? FWD_ROWS == 1 : FWD_ROWS == ROWS, "one forward pass per row group");
+    auto prod = [&](int r, int ab) { return ab < 3 ? W + (r * 6 + ab) * SP : S + r * STG + (ab - 3) * SP; };
 #pragma unroll 1
     for (int r0 = 0; r0 < ROWS; r0 += FWD_ROWS) {
-      const int t = tid % M, ab = (tid / M) % 6, r = r0 + tid / (6 * M);
-      // pairs 00 01 02 11 12 22
-      const int ca = (ab >= 3) + (ab >= 5), cb = ab < 3 ? ab : (ab < 5 ? ab - 2 : 2);
-      const C* Za = S + r * STG + ca * SP;
-      const C* Zb = S + r * STG + cb * SP;
-      C v[16];
+      {
+        // forward stage A: products fused into the loads
+        const int t = tid % M, ab = (tid / M) % 6, r = r0 + tid / (6 * M);
+        // pairs 00 01 02 11 12 22
+        const int ca = (ab >= 3) + (ab >= 5), cb = ab < 3 ? ab : (ab < 5 ? ab - 2 : 2);
+        const C* Za = W + (r * 6 + 3 + ca) * SP;
+        const C* Zb = W + (r * 6 + 3 + cb) * SP;
+        C v[16];
 #pragma unroll
-      for (int q = 0; q < 16; ++q) {
-        const int x = pp16(t + M * q);
-        const C za = Za[x], zb = Zb[x];
-        v[q] = cmk(za.x * zb.x, za.y * zb.y);
+        for (int q = 0; q < 16; ++q) {
+          const int x = pp16(t + M * q);
+          const C za = Za[x], zb = Zb[x];
+          v[q] = cmk(za.x * zb.x, za.y * zb.y);
+        }
+        dft16<-1>(v);
+        C* Wp = prod(r, ab);
+#pragma unroll
+        for (int q = 0; q < 16; ++q) Wp[pp16(16 * t + q)] = v[q];
       }
-      dft16<-1>(v);
-      C* Wp = W + (r * 6 + ab) * SP;
-#pragma unroll
-      for (int q = 0; q < 16; ++q) Wp[pp16(16 * t + q)] = v[q];
-    }
-    __syncthreads();
+      __syncwarp();
 
-    // ---- forward stage B, r2c unpack through the partner lane, stores to HBM
-    if constexpr (X::PAIR) {
-#pragma unroll 1
-     for (int r = 0; r < ROWS; ++r) {
-      const int lane = tid & 31, ab = tid >> 5, j = lane & 15, h = lane >> 4;
-      const C* Wp = W + (r * 6 + ab) * SP;
-      C v[16];
+      // forward stage B, r2c unpack through the partner lane, stores to HBM
+      if constexpr (X::PAIR) {
+        const int r = r0;
+        const int lane = tid & 31, ab = tid >> 5, j = lane & 15, h = lane >> 4;
+        const C* Wp = prod(r, ab);
+        C v[16];
 #pragma unroll
-      for (int i = 0; i < 16; ++i) {
-        const int rr = 2 * i + h;
-        v[i] = cmul(Wp[pp16(j + 16 * rr)], tw2[rr * 16 + j]);
-      }
-      dft16<-1>(v);
-      if (h) {
+        for (int i = 0; i < 16; ++i) {
+          const int rr = 2 * i + h;
+          v[i] = cmul(Wp[pp16(j + 16 * rr)], tw2[rr * 16 + j]);
+        }
+        dft16<-1>(v);
+        if (h) {
 #pragma unroll
-        for (int q = 1; q < 16; ++q) v[q] = cmul(v[q], tw2[16 * 16 + q]);
-      }
+          for (int q = 1; q < 16; ++q) v[q] = cmul(v[q], tw2[16 * 16 + q]);
+        }
 #pragma unroll
-      for (int q = 0; q < 16; ++q) {
-        const C o = shfl2_xor(v[q], 16);
-        v[q] = h ? csub(o, v[q]) : cadd(v[q], o);  // X(j + 16 (q + 16 h))
-      }
-      const int partner = ((16 - j) & 15) + 16 * (1 - h);
-      const long long row = it * ROWS + r;
-      C* o0 = work + (long long)(2 * ab) * g.field + row * g.pitch;
-      C* o1 = o0 + g.field;
+        for (int q = 0; q < 16; ++q) {
+          const C o = shfl2_xor(v[q], 16);
+          v[q] = h ? csub(o, v[q]) : cadd(v[q], o);  // X(j + 16 (q + 16 h))
+        }
+        const int partner = ((16 - j) & 15) + 16 * (1 - h);
+        const long long row = it * ROWS + r;
+        C* o0 = work + (long long)(2 * ab) * g.field + row * g.pitch;
+        C* o1 = o0 + g.field;
 #pragma unroll
-      for (int i = 0; i < 16; ++i) {
-        const C send = j == 0 ? v[(16 - i) & 15] : v[15 - i];
-        const C recv = shfl2(send, partner);
-        const C zm = (j == 0 && i == 0) ? v[0] : recv;
-        const int kk = j + 16 * (16 * h + i);
-        if (kk <= NH) {
-          C A, B;
-          unpack_pair(v[i], zm, &A, &B);
-          o0[kk] = A;
-          o1[kk] = B;
-          if (kk == NH) {
-            nyq_p0 += A.x;
-            nyq_ps += B.x;
+        for (int i = 0; i < 16; ++i) {
+          const C send = j == 0 ? v[(16 - i) & 15] : v[15 - i];
+          const C recv = shfl2(send, partner);
+          const C zm = (j == 0 && i == 0) ? v[0] : recv;
+          const int kk = j + 16 * (16 * h + i);
+          if (kk <= NH) {
+            C A, B;
+            unpack_pair(v[i], zm, &A, &B);
+            o0[kk] = A;
+            o1[kk] = B;
+            if (kk == NH) {
+              nyq_p0 += A.x;
+              nyq_ps += B.x;
+            }
           }
         }
-      }
-     }
-    } else {
-      const int j = tid & 15, sq = tid >> 4, r = sq / 6, ab = sq % 6;
-      const C* Wp = W + (r * 6 + ab) * SP;
-      C v[16];
+      } else {
+        const int j = tid & 15, sq = tid >> 4, r = sq / 6, ab = sq % 6;
+        const C* Wp = prod(r, ab);
+        C v[16];
 #pragma unroll
-      for (int q = 0; q < 16; ++q) v[q] = q == 0 ? Wp[pp16(j)] : cmul(Wp[pp16(j + 16 * q)], tw2[q * 16 + j]);
-      dft16<-1>(v);
-      const int lane = tid & 31;
-      const int partner = (lane & 16) + ((16 - j) & 15);
-      const long long row = it * ROWS + r;
-      C* o0 = work + (long long)(2 * ab) * g.field + row * g.pitch;
-      C* o1 = o0 + g.field;
+        for (int q = 0; q < 16; ++q) v[q] = q == 0 ? Wp[pp16(j)] : cmul(Wp[pp16(j + 16 * q)], tw2[q * 16 + j]);
+        dft16<-1>(v);
+        const int lane = tid & 31;
+        const int partner = (lane & 16) + ((16 - j) & 15);
+        const long long row = it * ROWS + r;
+        C* o0 = work + (long long)(2 * ab) * g.field + row * g.pitch;
+        C* o1 = o0 + g.field;
 #pragma unroll
-      for (int q = 0; q < 16; ++q) {
-        const C recv = shfl2(v[15 - q], partner);
-        const C zm = j == 0 ? v[(16 - q) & 15] : recv;
-        const int kk = j + 16 * q;
-        if (kk <= NH) {
-          C A, B;
-          unpack_pair(v[q], zm, &A, &B);
-          o0[kk] = A;
-          o1[kk] = B;
-          if (kk == NH) {
-            nyq_p0 += A.x;
-            nyq_ps += B.x;
+        for (int q = 0; q < 16; ++q) {
+          const C recv = shfl2(v[15 - q], partner);
+          const C zm = j == 0 ? v[(16 - q) & 15] : recv;
+          const int kk = j + 16 * q;
+          if (kk <= NH) {
+            C A, B;
+            unpack_pair(v[q], zm, &A, &B);
+            o0[kk] = A;
+            o1[kk] = B;
+            if (kk == NH) {
+              nyq_p0 += A.x;
+              nyq_ps += B.x;
+            }
           }
         }
       }
     }
-    __syncthreads();
-    if (tid == 0 && it + 2LL * gridDim.x < niter) issue(it + 2LL * gridDim.x, b);
+    // the staging rows were written through st.shared; order that before the bulk copy
+    // that refills them after the next row's barrier
+    fence_proxy_async_smem();
   }
   // per-CTA Nyquist partials, fixed order: [field][cta]
   if constexpr (X::PAIR) {
