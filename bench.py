@@ -44,6 +44,33 @@ DT = 1e-3
 # + u + g in, u + g out; g is not read in the first stage, hence 23 on average).
 PASS_BYTES_S = {"p1_zinv_phase": 9, "p2_yinv": 12, "p3_xpass": 18, "p3_nyq": 0,
                 "p4_yfwd": 24, "p5_zfwd": 24, "p5_sweep": 23}
+
+
+def live_fraction(n, w):
+    """Fraction L of the z-pencil column-block tiles (my, mx block of 128 bytes) that hold a
+    mode inside the sphere |k| <= N/2; the sphere pruning skips the rest."""
+    tw = 128 // (2 * w)
+    ncb = (n // 2 + tw - 1) // tw
+    live = 0
+    for my in range(n):
+        m = my if my <= n // 2 else my - n
+        live += sum(1 for cb in range(ncb) if 4 * ((cb * tw) ** 2 + m * m) <= n * n)
+    return live / (n * ncb)
+
+
+def pruned_pass_bytes(n, w):
+    """Per-launch algorithmic bytes (units of S) with the sphere pruning: the fused forward z
+    + sweep loads, transforms and sweeps only the live tiles."""
+    L = live_fraction(n, w)
+    b = dict(PASS_BYTES_S)
+    b["p5_sweep"] = 23 * L
+    return b, L
+
+
+def step_bytes_s(L):
+    """Bytes per RK3 step in units of S: 3 x (P1 9, P2 12, P3 18, P4 24, P5 24L), which is 261
+    without pruning (L = 1)."""
+    return 189 + 72 * L
 # kernels per RK3 stage at N = 512: P1, P2, P3, P4, the (N/2,0,0) mode, fused P5
 LAUNCHES_PER_STEP = 3 * 6
 # DRAM traffic per launch per grid point (dram__bytes_read.sum + dram__bytes_write.sum) from
@@ -263,16 +290,19 @@ def measure_form(args, n, precision, local, pg):
     prof = s.profile_passes(DT, 1)
     w = 8 if precision == 0 else 4
     S = n ** 3 * w
+    pass_bytes, L = pruned_pass_bytes(n, w)
     top = max(prof, key=prof.get)
-    achieved = PASS_BYTES_S[top] * S / (prof[top] / 1e3) / 1e9
+    achieved = pass_bytes[top] * S / (prof[top] / 1e3) / 1e9
     peak, peak_kind = load_peaks()
     traffic_table = TRAFFIC_PER_POINT if precision == 0 else TRAFFIC_PER_POINT_FP32
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "traffic": (traffic_table[top] * n ** 3) if top in traffic_table else None,
             "kernel": top, "peak_source": f"hbm_gbs {peak_kind}",
-            "algorithmic_bytes_per_launch": PASS_BYTES_S[top] * S, "mean_launch_ms": prof[top]}
+            "algorithmic_bytes_per_launch": pass_bytes[top] * S, "mean_launch_ms": prof[top]}
     return s, {"value": value, "ms_per_step": ms_max / args.steps, "clocks": clocks, "roofline": roof,
-               "passes_ms_per_stage": prof, "model_roofline_frac": value / (peak / (261 * w)),
+               "passes_ms_per_stage": prof, "live_tile_fraction": L,
+               "model_bytes_per_point_step": step_bytes_s(L) * w,
+               "model_roofline_frac": value / (peak / (step_bytes_s(L) * w)),
                "steps_done": args.warmup + args.steps + 1}
 
 
@@ -365,6 +395,8 @@ def run_b200(args, world, rank, local, pg):
             "roofline": r["roofline"],
             "passes_ms_per_stage": r["passes_ms_per_stage"],
             "model_roofline_frac": r["model_roofline_frac"],
+            "model_bytes_per_point_step": r["model_bytes_per_point_step"],
+            "live_tile_fraction": r["live_tile_fraction"],
             "e2e": e2e,
         }
         if "fp64" in results and head != "fp64":

@@ -73,6 +73,7 @@ SIGNATURES = {
     "sns_dump_velocity": (C.c_int, [_H, _DPP]),
     "sns_set_viscosity": (C.c_int, [_H, C.c_double]),
     "sns_set_nonlinear_form": (C.c_int, [_H, C.c_int]),
+    "sns_set_sphere_pruning": (C.c_int, [_H, C.c_int]),
     "sns_launch_config": (C.c_int, [_H, C.POINTER(C.c_int), C.c_int]),
     "sns_grid_size": (C.c_int, [_H]),
     "sns_device_bytes": (C.c_size_t, [_H]),
@@ -256,6 +257,10 @@ class Solver:
     def set_nonlinear_form(self, form: int):
         """0: the reference's conservative form (default), 1: the rotational form u x omega."""
         self._check(self.lib.sns_set_nonlinear_form(self.h, form))
+
+    def set_sphere_pruning(self, enabled: bool):
+        """Skip the z-pencil tiles outside the sphere |k| <= N/2 (default on; bitwise neutral)."""
+        self._check(self.lib.sns_set_sphere_pruning(self.h, 1 if enabled else 0))
 
     def device_bytes(self) -> int:
         return int(self.lib.sns_device_bytes(self.h))

@@ -102,6 +102,14 @@ struct sns_handle {
   // true when the state's mx = N/2 plane is zero off (N/2,0,0), as every masked state is;
   // then the passes skip that column and take the Nyquist mode from the state directly
   bool nyq_clean = true;
+  // Sphere pruning.  live: the (my * ncb + cb) column-block tiles of the z pencils with a mode
+  // inside the sphere |k| <= N/2 (4 ((cb * TW)^2 + my^2) <= N^2, ncb = tiles_data()); the
+  // others hold only modes that every RK stage zeroes.  sphere_clean: u is known to be exactly
+  // zero outside the sphere (true after any RK stage, false after the state is set).
+  int* live = nullptr;
+  int nlive = 0;
+  bool sphere_clean = false;
+  bool prune = true;  // sns_set_sphere_pruning
   std::string err;
 
   char* u() const { return state; }
@@ -261,7 +269,7 @@ CUtensorMap make_field_map(void* base, int nf, int axis, const sns::Geom& g, int
 }
 
 sns::TmaArgs tma_args(sns_handle* h, int f_in0, int nf, int ncb, void* out, int f_out0, double scale) {
-  sns::TmaArgs a;
+  sns::TmaArgs a{};
   a.f_in0 = f_in0;
   a.nf = nf;
   a.ncb = ncb;
@@ -368,6 +376,21 @@ void run_stage(sns_handle* h, char* u_src, char* g_buf, int stage, double dt, in
   cudaStream_t st = h->stream;
   const int tiles_in = h->nyq_clean ? h->tiles_data() : h->tiles_all();
   const int f_src = (int)((size_t)(u_src - h->state) / h->fbytes);  // u (0) or the g slot (3)
+  const bool fused = h->p5_grid > 0;
+  // Sphere pruning (RK update with the fused P5 only).  A column-block tile (my, cb) outside
+  // the disk 4 ((cb * TW)^2 + my^2) <= N^2 holds only modes outside the sphere: u is zero
+  // there before the stage (every stage's sweep zeroes those modes, so stages 1 and 2 may
+  // rely on stage 0; stage 0 relies on the handle's flag, and never inside a graph capture,
+  // where the graph may later be replayed on a new state) and the stage leaves it zero.  So
+  // P5 neither loads, transforms nor sweeps these tiles (their forward-z inputs are never
+  // needed); every other value is computed as without pruning.
+  bool capturing = false;
+  {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    capturing = cudaStreamIsCapturing(st, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone;
+  }
+  const bool prune = h->prune && fused && mode == 0 && h->nyq_clean && h->nlive > 0 &&
+                     (stage > 0 || (h->sphere_clean && !capturing));
   mark(pm, 0, st);
   o->yz_tma(h->map_state_z, 2, +1, 1, tma_args(h, f_src, 3, tiles_in, h->work, 0, h->inv_size()), h->tw, h->phase,
             g, h->tma_grid, st);
@@ -390,15 +413,14 @@ void run_stage(sns_handle* h, char* u_src, char* g_buf, int stage, double dt, in
   o->yz_tma(h->map_work_y, 1, -1, 0, tma_args(h, 0, 12, h->tiles_data(), h->work, 0, 1.0), h->tw, h->phase, g,
             h->tma_grid, st);
   mark(pm, 5, st);
-  const bool fused = h->p5_grid > 0;
   if (!fused)
     o->yz_tma(h->map_work_z, 2, -1, 0, tma_args(h, 0, 12, h->tiles_data(), h->work, 0, 1.0), h->tw, h->phase, g,
               h->tma_grid, st);
   mark(pm, 6, st);
   const sns::SweepArgs a = stage_args(h, stage, dt, mode);
   if (fused)
-    o->p5(h->map_work_z, u_src, g_buf, rhs_out, h->nyq_part, nparts, h->tw, h->phase, a, h->tiles_data(), g,
-          h->p5_grid, h->err_word, st);
+    o->p5(h->map_work_z, u_src, g_buf, rhs_out, h->nyq_part, nparts, h->tw, h->phase, a, h->tiles_data(),
+          prune ? h->live : nullptr, prune ? h->nlive : 0, g, h->p5_grid, h->err_word, st);
   else
     o->sweep(h->work, u_src, g_buf, rhs_out, h->nyq_part, nparts, h->phase, a, g, st);
   mark(pm, 7, st);
@@ -407,7 +429,8 @@ void run_stage(sns_handle* h, char* u_src, char* g_buf, int stage, double dt, in
 void step_once(sns_handle* h, double dt) {
   for (int s = 0; s < 3; ++s) {
     run_stage(h, h->u(), h->gb(), s, dt, 0, nullptr, nullptr);
-    h->nyq_clean = true;  // the sweep zeroes the plane mx = N/2 off (N/2,0,0)
+    h->nyq_clean = true;     // the sweep zeroes the plane mx = N/2 off (N/2,0,0)
+    h->sphere_clean = true;  // and every mode outside the sphere
   }
 }
 
@@ -490,6 +513,7 @@ void release(sns_handle* h) {
   cudaFree(h->tw2);
   cudaFree(h->nyq_part);
   cudaFree(h->xf);
+  cudaFree(h->live);
   if (h->ev0) cudaEventDestroy(h->ev0);
   if (h->ev1) cudaEventDestroy(h->ev1);
   if (h->stream) cudaStreamDestroy(h->stream);
@@ -541,7 +565,7 @@ const char* sns_version(void) { return "sns_b200 0.2 (sm_100a, fp64 plain form, 
 size_t sns_bytes_required(int n, int precision) {
   if (n <= 0 || (precision != SNS_PRECISION_FP64 && precision != SNS_PRECISION_FP32)) return 0;
   return 18 * field_bytes(n, precision) + partial_slots(n) * sizeof(double) +
-         (size_t)(4 * n + 64) * complex_bytes(precision);
+         (size_t)(4 * n + 64) * complex_bytes(precision) + (size_t)n * (n / 16 + 1) * sizeof(int);
 }
 
 int sns_create(int n, double nu, int precision, int viscous_mode, uint64_t seed, double pert_amp, int pert_kmax,
@@ -641,6 +665,22 @@ int sns_create(int n, double nu, int precision, int viscous_mode, uint64_t seed,
         for (int j = 0; j < 16; ++j) t2[(size_t)r * 16 + j] = tw[(size_t)(r * j) % n];
       upload_table(h->tw2, t2, precision, h->stream);
     }
+    {
+      // live column-block tiles of the sphere pruning, in (my, cb) order
+      const int ncb = h->tiles_data(), tcw = h->tcols();
+      std::vector<int> lv;
+      for (int my = 0; my < n; ++my) {
+        const long long m = my <= n / 2 ? my : my - n;
+        for (int cb = 0; cb < ncb; ++cb) {
+          const long long mx0 = (long long)cb * tcw;
+          if (4 * (mx0 * mx0 + m * m) <= (long long)n * n) lv.push_back(my * ncb + cb);
+        }
+      }
+      h->nlive = (int)lv.size();
+      alloc((void**)&h->live, lv.size() * sizeof(int));
+      ck(cudaMemcpyAsync(h->live, lv.data(), lv.size() * sizeof(int), cudaMemcpyHostToDevice, h->stream), "live");
+      ck(cudaStreamSynchronize(h->stream), "live");
+    }
     h->map_state_z = make_field_map(h->state, 6, 2, h->g, h->cbytes);
     h->map_work_y = make_field_map(h->work, 12, 1, h->g, h->cbytes);
     h->map_work_z = make_field_map(h->work, 12, 2, h->g, h->cbytes);
@@ -702,6 +742,13 @@ int sns_set_viscosity(sns_handle* h, double nu) {
   }
   h->nu = nu;
   return SNS_OK;
+}
+
+int sns_set_sphere_pruning(sns_handle* h, int enabled) {
+  return guarded(h, [&] {
+    if (enabled != 0 && enabled != 1) throw SnsError(SNS_ERR_INVALID, "enabled must be 0 or 1");
+    h->prune = enabled == 1;
+  });
 }
 
 int sns_set_nonlinear_form(sns_handle* h, int form) {
@@ -868,6 +915,7 @@ int sns_set_state(sns_handle* h, const double* const uhat_full[3]) {
       sync(h, "sns_set_state");
     }
     h->nyq_clean = !dirty;
+    h->sphere_clean = false;
   });
 }
 
@@ -961,6 +1009,8 @@ int sns_profile_passes(sns_handle* h, double dt, int nsteps, double* pass_ms) {
     for (int s = 0; s < nsteps; ++s) {
       for (int st = 0; st < 3; ++st) {
         run_stage(h, h->u(), h->gb(), st, dt, 0, nullptr, nullptr, &pm);
+        h->nyq_clean = true;
+        h->sphere_clean = true;
         sync(h, "sns_profile_passes");
         for (int i = 0; i < SNS_NUM_PASSES; ++i) {
           float ms = 0.f;

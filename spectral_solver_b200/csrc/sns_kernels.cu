@@ -1158,7 +1158,8 @@ template <int N, class C>
 __global__ void __launch_bounds__(nt_p5<N>(), tma_minb<N>())
 k_p5(const __grid_constant__ CUtensorMap map, C* __restrict__ u, C* __restrict__ gbuf,
      C* __restrict__ rhs, const double* __restrict__ nyq_part, int nparts, const C* __restrict__ tw,
-     const C* __restrict__ phase, SweepArgs a, int ncb, Geom g, int* err) {
+     const C* __restrict__ phase, SweepArgs a, int ncb, const int* __restrict__ live, int nlive, Geom g,
+     int* err) {
   constexpr int NT = nt_p5<N>();
   constexpr int BR = box_rows<N>();
   constexpr int NBOX = N / BR;
@@ -1200,13 +1201,21 @@ k_p5(const __grid_constant__ CUtensorMap map, C* __restrict__ u, C* __restrict__
   const uint32_t tq = tbase + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)((warp >> 2) * 4 * CW);
   const bool load_g = a.stage > 0;
 
-  const long long ntiles = (long long)ncb * N;  // (cb, my)
+  // tiles (cb, my), index my * ncb + cb (at most N x (N/16 + 1): 32-bit); with a live list
+  // only the listed ones
+  const long long ntiles = live ? (long long)nlive : (long long)ncb * N;
+  auto tile_of = [&](long long t, int& cb, int& my) {
+    const int idx = live ? __ldg(&live[t]) : (int)t;
+    my = idx / ncb;
+    cb = idx - my * ncb;
+  };
   const long long mytiles = blockIdx.x < ntiles ? (ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
   const long long nunits = 12 * mytiles;
   auto issue = [&](long long ul, int b) {
     const long long t = blockIdx.x + (ul / 12) * gridDim.x;
     const int f = (int)(ul % 12);
-    const int cb = (int)(t % ncb), my = (int)(t / ncb);
+    int cb, my;
+    tile_of(t, cb, my);
     C* dst = b ? in1 : in0;
     mbar_arrive_expect_tx(&bars[b], kTileBytes);
 #pragma unroll
@@ -1233,7 +1242,8 @@ k_p5(const __grid_constant__ CUtensorMap map, C* __restrict__ u, C* __restrict__
     const C* IN = b ? in1 : in0;
     const long long t = blockIdx.x + (ul / 12) * gridDim.x;
     const int f = (int)(ul % 12);
-    const int cb = (int)(t % ncb), my = (int)(t / ncb);
+    int cb, my;
+    tile_of(t, cb, my);
     const int mx0 = cb * TW;
     // Each radix butterfly of the last stage hands its R modes to the sink: column
     // s = b % TW (b = tid + i*NT), z index (j/NS)*NS*R + j%NS + r*NS with j = b / TW; mode
@@ -1725,12 +1735,12 @@ struct Launch {
     }
   }
   static void p5(const CUtensorMap& map, void* u, void* gbuf, void* rhs, const double* nyq_part, int nparts,
-                 const void* tw, const void* phase, SweepArgs a, int ncb, Geom g, int grid, int* err,
-                 cudaStream_t st) {
+                 const void* tw, const void* phase, SweepArgs a, int ncb, const int* live, int nlive, Geom g,
+                 int grid, int* err, cudaStream_t st) {
     if constexpr (N == 128 || N == 256 || N == 512) {
       k_nyq_mode<N, C><<<1, 32, 0, st>>>(F(u), F(gbuf), F(rhs), nyq_part, nparts, F(phase), a, g);
       k_p5<N, C><<<grid, nt_p5<N>(), tma_smem<N, C>(), st>>>(map, F(u), F(gbuf), F(rhs), nyq_part, nparts, F(tw),
-                                                              F(phase), a, ncb, g, err);
+                                                              F(phase), a, ncb, live, nlive, g, err);
     }
   }
   // Persistent grid of the fused P5 (0: this size runs forward z + sweep as two kernels).

@@ -90,9 +90,11 @@ struct Ops {
   void (*xpass2)(void* work, const void* unyq, const void* phase, double scale, int nyq_scalar, double* nyq_part,
                  const void* tw2, Geom g, int grid, int* err, cudaStream_t st);
   int (*xpass2_grid)(int nsm);
-  // fused forward z pass + k-space sweep (N = 128, 256, 512), TMA-fed, accumulators in TMEM
+  // fused forward z pass + k-space sweep (N = 128, 256, 512), TMA-fed, accumulators in TMEM;
+  // `live` (nlive entries of my * ncb + cb) restricts it to those tiles, null: all
   void (*p5)(const CUtensorMap& map, void* u, void* gbuf, void* rhs, const double* nyq_part, int nparts,
-             const void* tw, const void* phase, SweepArgs a, int ncb, Geom g, int grid, int* err, cudaStream_t st);
+             const void* tw, const void* phase, SweepArgs a, int ncb, const int* live, int nlive, Geom g, int grid,
+             int* err, cudaStream_t st);
   int (*p5_grid)(int nsm);
   // rotational form: omega_hat = i k x u_hat (3 fields); the x pass forming u x omega on both
   // grids (12 inputs -> 6 outputs in work fields 0..5); the sweep combining the two grids

@@ -59,6 +59,7 @@ def test_null_handle_calls(lib):
     assert lib.sns_step(None, 1e-3, 1) == 1
     assert lib.sns_debug_fail_after(None, 1) == 1
     assert lib.sns_set_viscosity(None, 1.0) == 1
+    assert lib.sns_set_sphere_pruning(None, 1) == 1
     assert lib.sns_grid_size(None) == 0
     assert lib.sns_autotune(None, 1, None, None) == 1
     assert lib.sns_batch_step(None, 1) == 1
