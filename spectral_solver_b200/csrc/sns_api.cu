@@ -105,7 +105,8 @@ struct sns_handle {
   // Sphere pruning.  live: the (my * ncb + cb) column-block tiles of the z pencils with a mode
   // inside the sphere |k| <= N/2 (4 ((cb * TW)^2 + my^2) <= N^2, ncb = tiles_data()); the
   // others hold only modes that every RK stage zeroes.  sphere_clean: u is known to be exactly
-  // zero outside the sphere (true after any RK stage, false after the state is set).
+  // zero outside the sphere (after creation and after any RK stage that ran, not one only
+  // captured into a graph; false after the state is set).
   int* live = nullptr;
   int nlive = 0;
   bool sphere_clean = false;
@@ -308,6 +309,12 @@ inline void mark(PassMarks* pm, int i, cudaStream_t st) {
   if (pm && pm->on) cudaEventRecord(pm->ev[i], st);
 }
 
+// Is `st` being captured into a graph (launches recorded now, run later)?
+bool capturing(cudaStream_t st) {
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  return cudaStreamIsCapturing(st, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone;
+}
+
 sns::SweepArgs stage_args(const sns_handle* h, int stage, double dt, int mode) {
   sns::SweepArgs a{};
   a.nu = h->nu;
@@ -384,13 +391,8 @@ void run_stage(sns_handle* h, char* u_src, char* g_buf, int stage, double dt, in
   // where the graph may later be replayed on a new state) and the stage leaves it zero.  So
   // P5 neither loads, transforms nor sweeps these tiles (their forward-z inputs are never
   // needed); every other value is computed as without pruning.
-  bool capturing = false;
-  {
-    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
-    capturing = cudaStreamIsCapturing(st, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone;
-  }
   const bool prune = h->prune && fused && mode == 0 && h->nyq_clean && h->nlive > 0 &&
-                     (stage > 0 || (h->sphere_clean && !capturing));
+                     (stage > 0 || (h->sphere_clean && !capturing(st)));
   mark(pm, 0, st);
   o->yz_tma(h->map_state_z, 2, +1, 1, tma_args(h, f_src, 3, tiles_in, h->work, 0, h->inv_size()), h->tw, h->phase,
             g, h->tma_grid, st);
@@ -427,10 +429,12 @@ void run_stage(sns_handle* h, char* u_src, char* g_buf, int stage, double dt, in
 }
 
 void step_once(sns_handle* h, double dt) {
+  const bool deferred = capturing(h->stream);  // a captured graph runs later, on whatever state
   for (int s = 0; s < 3; ++s) {
     run_stage(h, h->u(), h->gb(), s, dt, 0, nullptr, nullptr);
-    h->nyq_clean = true;     // the sweep zeroes the plane mx = N/2 off (N/2,0,0)
-    h->sphere_clean = true;  // and every mode outside the sphere
+    h->nyq_clean = true;  // the sweep zeroes the plane mx = N/2 off (N/2,0,0)
+    // and every mode outside the sphere, once the stage has run
+    if (!deferred) h->sphere_clean = true;
   }
 }
 
@@ -708,6 +712,7 @@ int sns_create(int n, double nu, int precision, int viscous_mode, uint64_t seed,
       ck(cudaStreamSynchronize(h->stream), "perturbation");
     }
     sns::launch_project_truncate(h->u(), precision, h->g, h->stream);
+    h->sphere_clean = true;  // project_truncate zeroed every mode outside the sphere
     ck(cudaMemsetAsync(h->work, 0, 12 * fb, h->stream), "memset");
     sync(h, "sns_create");
   } catch (const SnsError& e) {
