@@ -74,16 +74,15 @@ def step_bytes_s(L):
     return 189 + 72 * L
 # kernels per RK3 stage at N = 512: P1, P2, P3, P4, the (N/2,0,0) mode, fused P5
 LAUNCHES_PER_STEP = 3 * 6
-# DRAM traffic per launch per grid point (dram__bytes_read.sum + dram__bytes_write.sum) from
-# single-launch ncu captures at 256^3 (profiles/k_*_256_fp64.txt; k_p5 with the sphere
-# pruning, whose live fraction is 0.81 at 256^3 and 0.80 at 512^3), scaled by N^3: traffic
-# grows with the grid points, and the 512^3 workload is too large for a full capture.
-TRAFFIC_PER_POINT = {"p5_sweep": (2.027e9 + 0.629e9) / 256 ** 3, "p3_xpass": (0.868e9 + 1.578e9) / 256 ** 3,
+# DRAM traffic per launch per grid point (dram__bytes_read.sum + dram__bytes_write.sum).  The
+# x pass and the fused P5 were captured on the 512^3 bench workload itself (one-pass metrics;
+# profiles/taylor_green_512_dram_traffic.txt; P5 with the sphere pruning); the other passes
+# come from single-launch captures at 256^3 (profiles/k_*_256_fp64.txt), scaled by N^3.
+TRAFFIC_PER_POINT = {"p5_sweep": (16.716e9 + 5.166e9) / 512 ** 3, "p3_xpass": (6.696e9 + 12.928e9) / 512 ** 3,
                      "p4_yfwd": 3.268e9 / 256 ** 3, "p1_zinv_phase": 1.166e9 / 256 ** 3,
                      "p2_yinv": 1.582e9 / 256 ** 3}
-# The same for the FP32 precision form (profiles/k_p5_xpass2_256_fp32.txt: single-launch
-# captures at 256^3, scaled by N^3 like the FP64 figures).
-TRAFFIC_PER_POINT_FP32 = {"p3_xpass": (0.465e9 + 0.774e9) / 256 ** 3, "p5_sweep": (1.068e9 + 0.306e9) / 256 ** 3}
+# The same for the FP32 precision form.
+TRAFFIC_PER_POINT_FP32 = {"p3_xpass": (3.474e9 + 6.487e9) / 512 ** 3, "p5_sweep": (8.473e9 + 2.619e9) / 512 ** 3}
 
 
 def load_peaks():
