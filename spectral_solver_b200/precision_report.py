@@ -25,6 +25,27 @@ import numpy as np
 from ._lib import PRECISION_FP32, PRECISION_FP64, Solver
 
 
+def summarize(a, b, state32, state64):
+    """The report's figures from the two diagnostic series (rows t, E, eps, enstrophy; `a` the
+    FP32 form, `b` the FP64 form, same output times) and the two final spectral states."""
+    t = b[:, 0]
+
+    def gaps(mask):
+        dE = np.abs(a[mask, 1] - b[mask, 1])
+        dEps = np.abs(a[mask, 2] - b[mask, 2])
+        return {"max_abs_E": float(dE.max()), "max_rel_E": float(dE.max() / np.abs(b[mask, 1]).max()),
+                "max_abs_eps": float(dEps.max()), "max_rel_eps": float(dEps.max() / np.abs(b[mask, 2]).max())}
+
+    num = sum(float(np.sum(np.abs(x - y) ** 2)) for x, y in zip(state32, state64))
+    den = sum(float(np.sum(np.abs(y) ** 2)) for y in state64)
+    ip32, ip64 = int(np.argmax(a[:, 2])), int(np.argmax(b[:, 2]))
+    return {"whole_run": gaps(np.ones_like(t, dtype=bool)), "up_to_t9": gaps(t <= 9.0 + 1e-12),
+            "peak_eps": {"t_fp64": float(t[ip64]), "t_fp32": float(t[ip32]),
+                         "abs_dt": float(abs(t[ip32] - t[ip64])), "eps_fp64": float(b[ip64, 2]),
+                         "eps_fp32": float(a[ip32, 2])},
+            "final_velocity_rel_l2": (num / den) ** 0.5}
+
+
 def run(n=512, dt=1e-3, t_end=20.0, output_dt=0.1, reynolds=1600.0, seed=0, pert_amp=0.0, pert_kmax=0):
     per_out = max(1, int(round(output_dt / dt)))
     nsteps = int(round(t_end / dt))
@@ -50,24 +71,8 @@ def run(n=512, dt=1e-3, t_end=20.0, output_dt=0.1, reynolds=1600.0, seed=0, pert
             # keep the stored half (mx in [0, N/2]) of the final state: host memory at 512^3
             states[name] = [np.ascontiguousarray(c[..., : n // 2 + 1]) for c in s.get_state()]
         series[name] = np.array(rows)
-    a, b = series["fp32"], series["fp64"]
-    t = b[:, 0]
-
-    def gaps(mask):
-        dE = np.abs(a[mask, 1] - b[mask, 1])
-        dEps = np.abs(a[mask, 2] - b[mask, 2])
-        return {"max_abs_E": float(dE.max()), "max_rel_E": float(dE.max() / np.abs(b[mask, 1]).max()),
-                "max_abs_eps": float(dEps.max()), "max_rel_eps": float(dEps.max() / np.abs(b[mask, 2]).max())}
-
-    num = sum(float(np.sum(np.abs(x - y) ** 2)) for x, y in zip(states["fp32"], states["fp64"]))
-    den = sum(float(np.sum(np.abs(y) ** 2)) for y in states["fp64"])
-    ip32, ip64 = int(np.argmax(a[:, 2])), int(np.argmax(b[:, 2]))
-    report = {"n": n, "dt": dt, "t_end": t_end, "steps": nsteps, "reynolds": reynolds,
-              "whole_run": gaps(np.ones_like(t, dtype=bool)), "up_to_t9": gaps(t <= 9.0 + 1e-12),
-              "peak_eps": {"t_fp64": float(t[ip64]), "t_fp32": float(t[ip32]),
-                           "abs_dt": float(abs(t[ip32] - t[ip64])), "eps_fp64": float(b[ip64, 2]),
-                           "eps_fp32": float(a[ip32, 2])},
-              "final_velocity_rel_l2": (num / den) ** 0.5, "wall_s": walls}
+    report = summarize(series["fp32"], series["fp64"], states["fp32"], states["fp64"])
+    report.update({"n": n, "dt": dt, "t_end": t_end, "steps": nsteps, "reynolds": reynolds, "wall_s": walls})
     return report, series
 
 
