@@ -434,8 +434,8 @@ struct XP {
   static constexpr bool PAIR = (M == 32);          // radix 32 as two radix-16 halves + shuffle
   static constexpr int NH = N / 2;
   // rows per iteration: two where their staging fits the CTA budget (N = 256; N = 512 in
-  // FP32), so the inverse stages keep all 192 threads busy and one barrier sequence serves
-  // two rows
+  // FP32), so one barrier sequence serves two rows and, at N = 512, the inverse stages keep
+  // all 192 threads busy (96 at N = 256, one half-warp per FFT)
   static constexpr int ROWS = (N == 256 || sizeof(C) == 8) ? 2 : 1;
   static constexpr int SP = N + N / 16;            // padded sequence (one slot per 16)
   static constexpr int NT = 192;
@@ -506,12 +506,12 @@ k_xpass2(C* __restrict__ work, const C* __restrict__ unyq, const C* __restrict__
     const uint32_t parity = (uint32_t)(k >> 1) & 1u;
     if (tid == 0 && !mbar_wait_bounded(&bars[b], parity)) s_fail = 1;
     __syncthreads();
-    if (s_fail) {  // no other copy is in flight: the next row is issued after this wait
+    if (s_fail) {  // no other copy is in flight: the next row group is issued after this wait
       if (tid == 0) atomicExch(err, kErrTmaTimeout);
       return;
     }
     (void)mbar_try_wait(&bars[b], parity);
-    // every thread has finished the previous row, so its staging buffer takes the next one
+    // every thread has finished the previous row group, so its staging buffer takes the next
     if (tid == 0 && it + gridDim.x < niter) issue(it + gridDim.x, b ^ 1);
     C* S = stg + b * ROWS * STG;
 
