@@ -132,6 +132,18 @@ int sns_set_nonlinear_form(sns_handle* h, int form);
  * The results are bitwise those of the full computation; enabled = 0 runs every tile. */
 int sns_set_sphere_pruning(sns_handle* h, int enabled);
 
+/* Compensated state of the FP32 precision form (on by default there; no counterpart in the
+ * reference, whose FP32 build rounds u to FP32 after every stage).  Each complex value of u
+ * is kept as its FP32 value plus a bf16 pair holding the remainder, and the k-space sweep
+ * forms the RK update u += b*dt*g and the projection of u in FP64 from the two.  Without it
+ * the FP32 rounding of u drops the low bits of each stage's small increment, which over
+ * thousands of steps dominates the form's error against FP64.  Costs 3 words per mode of
+ * device memory and 6 words per mode of traffic in the sweep.  get_state returns the
+ * compensated value and set_state fills both parts, so a state round-trips exactly.
+ * Enabling it after it was off restarts the remainder at zero.  The FP64 form accepts 0
+ * only (SNS_ERR_UNSUPPORTED for 1). */
+int sns_set_compensation(sns_handle* h, int enabled);
+
 /* Persistent grids chosen at creation: out[0] TMA y/z passes, out[1] two-stage x pass
  * (0 = generic), out[2] fused forward-z + sweep (0 = two kernels), out[3] SM count. */
 int sns_launch_config(const sns_handle* h, int* out, int count);
@@ -253,14 +265,27 @@ const char* sns_server_last_error(const sns_server* s);
  * 48 64); larger grids return SNS_ERR_UNSUPPORTED.  The intermediate spectrum lives in one
  * fixed __device__ array (about 2.5 MiB) that every GPU loading the library holds until
  * exit and that all calls on a device share: calls whose GPU work overlaps race on it.
- * The first call on a device sets that array up (with the device current); make it before
- * any stream capture begins.  Errors: sns_last_error(NULL). */
+ * The first call on a device sets that array up (with the device current).  Every call
+ * returns after its work on `stream` finished (it synchronises that stream), so a stream
+ * that is being captured is refused with SNS_ERR_INVALID.  Errors: sns_last_error(NULL). */
 #define SNS_NOALLOC_MAX_N 64
 int sns_forward_r2c_noalloc(int n, const double* dev_physical, double* dev_spectral, void* stream);
 
 /* Test hook: the k-th following call into the handle fails with SNS_ERR_INJECTED
  * (k <= 0 disables).  Exercises the error paths without touching the GPU. */
 int sns_debug_fail_after(sns_handle* h, int k);
+
+/* Test hook: write `code` into the handle's device error word, where a pass kernel records a
+ * bounded wait that ran out (1 = a TMA tile did not land).  The next call that synchronises
+ * the handle reports it as SNS_ERR_CUDA and clears the word; the call after that runs
+ * normally.  Exercises the host side of the device error path without a device fault. */
+int sns_debug_set_error_word(sns_handle* h, int code);
+
+/* Test hook: one thread arms a shared-memory barrier for bytes no copy will deliver and
+ * polls it `polls` times (1 .. 2^22) as the pass kernels poll their tiles; *status receives
+ * 1 when the wait ran out (the pass kernels' timeout code), 0 if it landed.  Runs on the
+ * current device and synchronises it.  Errors: sns_last_error(NULL). */
+int sns_debug_bounded_wait(unsigned polls, int* status);
 
 #ifdef __cplusplus
 }

@@ -5,7 +5,7 @@ TEST INFRASTRUCTURE ONLY (used by tests and the CPU legs of ``bench.py``).
 The reference has no perturbed initial condition (its AVA path starts from the pure
 Taylor-Green field, ``ava_taylor_green_impl.hpp:796-817``).  The perturbation is new in
 this project and is specified once; the device library implements the same definition
-(``spectral_solver_b200/csrc/perturbation.cpp``) and the tests check the two agree.
+(``perturbation_entries`` in ``spectral_solver_b200/csrc/sns_api.cu``) and the tests check the two agree.
 
 Specification (half spectrum, reference full-layout flat index):
   * modes m = (mx, my, mz), mx in [0, N/2], my, mz signed in (-N/2, N/2], with

@@ -74,11 +74,14 @@ SIGNATURES = {
     "sns_set_viscosity": (C.c_int, [_H, C.c_double]),
     "sns_set_nonlinear_form": (C.c_int, [_H, C.c_int]),
     "sns_set_sphere_pruning": (C.c_int, [_H, C.c_int]),
+    "sns_set_compensation": (C.c_int, [_H, C.c_int]),
     "sns_launch_config": (C.c_int, [_H, C.POINTER(C.c_int), C.c_int]),
     "sns_grid_size": (C.c_int, [_H]),
     "sns_device_bytes": (C.c_size_t, [_H]),
     "sns_time_steps": (C.c_int, [_H, C.c_double, C.c_int, _DP]),
     "sns_debug_fail_after": (C.c_int, [_H, C.c_int]),
+    "sns_debug_set_error_word": (C.c_int, [_H, C.c_int]),
+    "sns_debug_bounded_wait": (C.c_int, [C.c_uint, C.POINTER(C.c_int)]),
     "sns_profile_passes": (C.c_int, [_H, C.c_double, C.c_int, _DP]),
     "sns_forward_r2c_noalloc": (C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
     "sns_batch_create": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_char_p, C.POINTER(C.c_void_p), _DP]),
@@ -261,6 +264,11 @@ class Solver:
     def set_sphere_pruning(self, enabled: bool):
         """Skip the z-pencil tiles outside the sphere |k| <= N/2 (default on; bitwise neutral)."""
         self._check(self.lib.sns_set_sphere_pruning(self.h, 1 if enabled else 0))
+
+    def set_compensation(self, enabled: bool):
+        """FP32 form: carry u as its FP32 value plus a bf16 remainder, the RK update formed in
+        FP64 (default on; the FP64 form accepts False only)."""
+        self._check(self.lib.sns_set_compensation(self.h, 1 if enabled else 0))
 
     def device_bytes(self) -> int:
         return int(self.lib.sns_device_bytes(self.h))

@@ -111,11 +111,17 @@ struct sns_handle {
   int nlive = 0;
   bool sphere_clean = false;
   bool prune = true;  // sns_set_sphere_pruning
+  // FP32 precision form: compensation words of u (3 fields of one 32-bit word per complex
+  // value, the index of u), so the RK update keeps the low bits the FP32 state drops;
+  // comp: in use (sns_set_compensation)
+  uint32_t* ulo = nullptr;
+  bool comp = false;
   std::string err;
 
   char* u() const { return state; }
   char* gb() const { return state + 3 * fbytes; }
   char* ucomp(int c) const { return state + (size_t)c * fbytes; }
+  uint32_t* locomp(int c) const { return comp ? ulo + (size_t)c * g.field : nullptr; }
   char* wf(int i) const { return work + (size_t)i * fbytes; }
   int tcols() const { return ops->tile_cols; }
   int tiles_data() const { return (g.nh + tcols() - 1) / tcols(); }  // columns [0, N/2)
@@ -142,6 +148,12 @@ void upload_table(void* dst, const std::vector<double2>& t, int precision, cudaS
     ck(cudaMemcpyAsync(dst, t.data(), t.size() * sizeof(double2), cudaMemcpyHostToDevice, st), "table upload");
     ck(cudaStreamSynchronize(st), "table upload");
   }
+}
+
+// Bytes of the compensation words of u (FP32 form): 3 fields of 4 bytes per complex value.
+size_t comp_bytes(int n, int precision) {
+  if (precision != SNS_PRECISION_FP32) return 0;
+  return (size_t)3 * n * n * sns::pitch_for(n, 8) * sizeof(uint32_t);
 }
 
 size_t partial_slots(int n) {
@@ -315,9 +327,11 @@ bool capturing(cudaStream_t st) {
   return cudaStreamIsCapturing(st, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone;
 }
 
-sns::SweepArgs stage_args(const sns_handle* h, int stage, double dt, int mode) {
+sns::SweepArgs stage_args(const sns_handle* h, int stage, double dt, int mode, const char* u_src) {
   sns::SweepArgs a{};
   a.nu = h->nu;
+  // the compensated update applies to the handle's own state only (not to sns_rhs inputs)
+  a.ulo = (h->comp && mode == 0 && u_src == h->u()) ? h->ulo : nullptr;
   a.stage = stage;
   a.mode = mode;
   a.dealias = 1;
@@ -367,7 +381,7 @@ void run_stage_rot(sns_handle* h, char* u_src, char* g_buf, int stage, double dt
   o->yz_tma(h->map_work_z, 2, -1, 0, tma_args(h, 0, 6, h->tiles_data(), h->work, 0, 1.0), h->tw, h->phase, g,
             h->tma_grid, st);
   mark(pm, 6, st);
-  o->sweep_rot(h->work, u_src, g_buf, rhs_out, h->nyq_part, h->phase, stage_args(h, stage, dt, mode), g, st);
+  o->sweep_rot(h->work, u_src, g_buf, rhs_out, h->nyq_part, h->phase, stage_args(h, stage, dt, mode, u_src), g, st);
   mark(pm, 7, st);
 }
 
@@ -419,7 +433,7 @@ void run_stage(sns_handle* h, char* u_src, char* g_buf, int stage, double dt, in
     o->yz_tma(h->map_work_z, 2, -1, 0, tma_args(h, 0, 12, h->tiles_data(), h->work, 0, 1.0), h->tw, h->phase, g,
               h->tma_grid, st);
   mark(pm, 6, st);
-  const sns::SweepArgs a = stage_args(h, stage, dt, mode);
+  const sns::SweepArgs a = stage_args(h, stage, dt, mode, u_src);
   if (fused)
     o->p5(h->map_work_z, u_src, g_buf, rhs_out, h->nyq_part, nparts, h->tw, h->phase, a, h->tiles_data(),
           prune ? h->live : nullptr, prune ? h->nlive : 0, g, h->p5_grid, h->err_word, st);
@@ -452,17 +466,18 @@ bool nyquist_plane_dirty(int n, const double* full) {
 
 // Upload a reference full-layout field into half field `dst` (optionally Hermitian part).
 // The N^3 complex doubles of a full-layout field fit in work fields 4..11 for either precision.
-void upload_full(sns_handle* h, const double* host, void* dst, int herm) {
+// With `lo` (FP32 form, compensated state) the remainder the FP32 value drops goes there.
+void upload_full(sns_handle* h, const double* host, void* dst, int herm, uint32_t* lo = nullptr) {
   double2* staging = reinterpret_cast<double2*>(h->wf(4));
   const size_t bytes = (size_t)h->n * h->n * h->n * sizeof(double2);
   ck(cudaMemcpyAsync(staging, host, bytes, cudaMemcpyHostToDevice, h->stream), "upload");
-  sns::launch_full_to_half(staging, dst, h->precision, herm, h->g, h->stream);
+  sns::launch_full_to_half(staging, dst, h->precision, herm, h->g, h->stream, lo);
 }
 
-void download_full(sns_handle* h, const void* src, double* host) {
+void download_full(sns_handle* h, const void* src, double* host, const uint32_t* lo = nullptr) {
   double2* staging = reinterpret_cast<double2*>(h->wf(4));
   const size_t bytes = (size_t)h->n * h->n * h->n * sizeof(double2);
-  sns::launch_half_to_full(src, h->precision, staging, h->g, h->stream);
+  sns::launch_half_to_full(src, h->precision, staging, h->g, h->stream, lo);
   ck(cudaMemcpyAsync(host, staging, bytes, cudaMemcpyDeviceToHost, h->stream), "download");
 }
 
@@ -518,6 +533,7 @@ void release(sns_handle* h) {
   cudaFree(h->nyq_part);
   cudaFree(h->xf);
   cudaFree(h->live);
+  cudaFree(h->ulo);
   if (h->ev0) cudaEventDestroy(h->ev0);
   if (h->ev1) cudaEventDestroy(h->ev1);
   if (h->stream) cudaStreamDestroy(h->stream);
@@ -568,7 +584,7 @@ const char* sns_version(void) { return "sns_b200 0.2 (sm_100a, fp64 plain form, 
 
 size_t sns_bytes_required(int n, int precision) {
   if (n <= 0 || (precision != SNS_PRECISION_FP64 && precision != SNS_PRECISION_FP32)) return 0;
-  return 18 * field_bytes(n, precision) + partial_slots(n) * sizeof(double) +
+  return 18 * field_bytes(n, precision) + comp_bytes(n, precision) + partial_slots(n) * sizeof(double) +
          (size_t)(4 * n + 64) * complex_bytes(precision) + (size_t)n * (n / 16 + 1) * sizeof(int);
 }
 
@@ -690,6 +706,12 @@ int sns_create(int n, double nu, int precision, int viscous_mode, uint64_t seed,
     h->map_work_z = make_field_map(h->work, 12, 2, h->g, h->cbytes);
     ck(cudaMemsetAsync(h->state, 0, 6 * fb, h->stream), "memset");
     ck(cudaMemsetAsync(h->work, 0, 12 * fb, h->stream), "memset");
+    if (precision == SNS_PRECISION_FP32) {
+      // the precision form carries u compensated (hi + lo); the initial state has lo = 0
+      alloc((void**)&h->ulo, comp_bytes(n, precision));
+      ck(cudaMemsetAsync(h->ulo, 0, comp_bytes(n, precision), h->stream), "memset");
+      h->comp = true;
+    }
     const auto tw = twiddle_table(n);
     const auto ph = phase_table(n);
     upload_table(h->tw, tw, precision, h->stream);
@@ -747,6 +769,22 @@ int sns_set_viscosity(sns_handle* h, double nu) {
   }
   h->nu = nu;
   return SNS_OK;
+}
+
+int sns_set_compensation(sns_handle* h, int enabled) {
+  return guarded(h, [&] {
+    if (enabled != 0 && enabled != 1) throw SnsError(SNS_ERR_INVALID, "enabled must be 0 or 1");
+    if (h->precision != SNS_PRECISION_FP32) {
+      if (enabled) throw SnsError(SNS_ERR_UNSUPPORTED, "the compensated state belongs to the FP32 precision form");
+      return;
+    }
+    if (enabled && !h->comp) {
+      // lo was not kept while off: the state restarts from its FP32 value
+      ck(cudaMemsetAsync(h->ulo, 0, comp_bytes(h->n, h->precision), h->stream), "memset");
+      sync(h, "sns_set_compensation");
+    }
+    h->comp = enabled == 1;
+  });
 }
 
 int sns_set_sphere_pruning(sns_handle* h, int enabled) {
@@ -875,6 +913,13 @@ int sns_autotune(sns_handle* h, int trial_steps, const char* cache_path, int* ou
   });
 }
 
+int sns_debug_set_error_word(sns_handle* h, int code) {
+  return guarded(h, [&] {
+    ck(cudaMemcpyAsync(h->err_word, &code, sizeof(int), cudaMemcpyHostToDevice, h->stream), "error word");
+    ck(cudaStreamSynchronize(h->stream), "error word");
+  });
+}
+
 int sns_debug_fail_after(sns_handle* h, int k) {
   if (h == nullptr) return SNS_ERR_INVALID;
   h->fail_after = k > 0 ? k : 0;
@@ -913,9 +958,10 @@ int sns_set_state(sns_handle* h, const double* const uhat_full[3]) {
   return guarded(h, [&] {
     if (!uhat_full || !uhat_full[0] || !uhat_full[1] || !uhat_full[2]) throw SnsError(SNS_ERR_INVALID, "null buffer");
     ck(cudaMemsetAsync(h->u(), 0, 3 * h->fbytes, h->stream), "memset");
+    if (h->comp) ck(cudaMemsetAsync(h->ulo, 0, comp_bytes(h->n, h->precision), h->stream), "memset");
     bool dirty = false;
     for (int c = 0; c < 3; ++c) {
-      upload_full(h, uhat_full[c], h->ucomp(c), 0);
+      upload_full(h, uhat_full[c], h->ucomp(c), 0, h->locomp(c));
       dirty = dirty || nyquist_plane_dirty(h->n, uhat_full[c]);
       sync(h, "sns_set_state");
     }
@@ -928,7 +974,7 @@ int sns_get_state(sns_handle* h, double* const uhat_full[3]) {
   return guarded(h, [&] {
     if (!uhat_full || !uhat_full[0] || !uhat_full[1] || !uhat_full[2]) throw SnsError(SNS_ERR_INVALID, "null buffer");
     for (int c = 0; c < 3; ++c) {
-      download_full(h, h->ucomp(c), uhat_full[c]);
+      download_full(h, h->ucomp(c), uhat_full[c], h->locomp(c));
       sync(h, "sns_get_state");
     }
   });

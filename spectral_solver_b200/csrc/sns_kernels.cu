@@ -762,12 +762,36 @@ __device__ __forceinline__ C pair_value(C p0, C ps, C phase, bool keep, int deal
 // projection of u (:994-1039) -- or the RHS itself in modes 1 and 2.
 template <class C>
 __device__ __forceinline__ void finish_mode(C r[3], int ix, int iy, int iz, int n, C uu[3], C gg[3],
-                                            bool load_g, C rr[3], const SweepArgs& a);
+                                            bool load_g, C rr[3], const SweepArgs& a, uint32_t lo[3]);
+
+// Compensated state of the FP32 precision form.  The RK update u += b*dt*g adds an
+// increment some 1e-3 of |u| at dt = 1e-3; rounding u to FP32 after every stage drops the
+// increment's low bits, and over thousands of steps that dominates the form's error.  So u
+// is carried as its stored FP32 value hi plus a remainder lo, one 32-bit word per complex
+// value holding two bf16 (re in the low half, im in the high half).  The sweep forms the
+// update in FP64 from hi + lo.  lo is the remainder U - hi rounded toward zero (to FP32,
+// then to bf16 by dropping mantissa bits), so |lo| stays below half an FP32 ulp of hi and
+// round-to-nearest(hi + lo) gives hi back: the pair decodes to an FP64 value and encodes
+// back to the same pair (exact state round trips through the host).
+__device__ __forceinline__ double2 comp_decode(float2 hi, uint32_t lo) {
+  const float lr = __uint_as_float(lo << 16), li = __uint_as_float(lo & 0xffff0000u);
+  return make_double2((double)hi.x + (double)lr, (double)hi.y + (double)li);
+}
+__device__ __forceinline__ float2 comp_encode(double2 U, uint32_t* lo) {
+  const float2 hi = make_float2(__double2float_rn(U.x), __double2float_rn(U.y));
+  // U - hi is exact in FP64 (the two are within a factor of two, or hi is zero)
+  const float lr = __double2float_rz(U.x - (double)hi.x), li = __double2float_rz(U.y - (double)hi.y);
+  uint32_t br = __float_as_uint(lr) & 0xffff0000u, bi = __float_as_uint(li) & 0xffff0000u;
+  if ((br & 0x7fffffffu) == 0u) br = 0u;  // no negative zeros: each value has one encoding
+  if ((bi & 0x7fffffffu) == 0u) bi = 0u;
+  *lo = (br >> 16) | bi;
+  return hi;
+}
 
 template <class C>
 __device__ __forceinline__ void sweep_mode(const ModeIn<C>& in, int ix, int iy, int iz, int n, C phase,
                                            C uu[3], C gg[3], bool load_g, C rr[3],
-                                           const SweepArgs& a) {
+                                           const SweepArgs& a, uint32_t lo[3]) {
   const int m2 = ix * ix + iy * iy + iz * iz;
   const bool keep = 4LL * m2 <= (long long)n * n;
   const int kv[3] = {ix, iy, iz};
@@ -780,12 +804,12 @@ __device__ __forceinline__ void sweep_mode(const ModeIn<C>& in, int ix, int iy, 
     r[pa[p]] = cadd(r[pa[p]], minus_i_k(value, kv[pb[p]]));
     if (pa[p] != pb[p]) r[pb[p]] = cadd(r[pb[p]], minus_i_k(value, kv[pa[p]]));
   }
-  finish_mode(r, ix, iy, iz, n, uu, gg, load_g, rr, a);
+  finish_mode(r, ix, iy, iz, n, uu, gg, load_g, rr, a, lo);
 }
 
 template <class C>
 __device__ __forceinline__ void finish_mode(C r[3], int ix, int iy, int iz, int n, C uu[3], C gg[3],
-                                            bool load_g, C rr[3], const SweepArgs& a) {
+                                            bool load_g, C rr[3], const SweepArgs& a, uint32_t lo[3]) {
   const int m2 = ix * ix + iy * iy + iz * iz;
   const bool keep = 4LL * m2 <= (long long)n * n;
   const double k2 = (double)m2;
@@ -813,6 +837,42 @@ __device__ __forceinline__ void finish_mode(C r[3], int ix, int iy, int iz, int 
     rr[1] = r[1];
     rr[2] = r[2];
     return;
+  }
+  if constexpr (sizeof(C) == 8) {
+    if (a.ulo != nullptr) {
+      // FP32 form with the compensated state: u = hi + lo updated and projected in FP64
+      double2 U[3];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        gg[c] = load_g ? cadd(cscale(gg[c], (float)a.ga), r[c]) : r[c];
+        U[c] = comp_decode(uu[c], lo[c]);
+        U[c] = make_double2(U[c].x + a.ub * (double)gg[c].x, U[c].y + a.ub * (double)gg[c].y);
+      }
+      if (a.visc_if) {
+        const double f = exp(-a.nu * k2 * a.if_tau);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          U[c] = make_double2(U[c].x * f, U[c].y * f);
+          gg[c] = cscale(gg[c], (float)f);
+        }
+      }
+      if (k2 > 0.0 && keep) {
+        const double2 dot = make_double2((U[0].x * ix + U[1].x * iy) + U[2].x * iz,
+                                         (U[0].y * ix + U[1].y * iy) + U[2].y * iz);
+        const double2 factor = make_double2(dot.x * (1.0 / k2), dot.y * (1.0 / k2));
+        const double kv[3] = {(double)ix, (double)iy, (double)iz};
+#pragma unroll
+        for (int c = 0; c < 3; ++c) uu[c] = comp_encode(make_double2(U[c].x - factor.x * kv[c],
+                                                                     U[c].y - factor.y * kv[c]), &lo[c]);
+      } else {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          uu[c] = czero<C>();
+          lo[c] = 0u;
+        }
+      }
+      return;
+    }
   }
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
@@ -861,12 +921,14 @@ k_sweep(const C* __restrict__ work, C* __restrict__ u, C* __restrict__ gbuf,
       in.ps[p] = work[(long long)(2 * p + 1) * g.field + idx];
     }
     C uu[3], gg[3], rr[3];
+    uint32_t lo[3] = {0u, 0u, 0u};
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       uu[c] = u[(long long)c * g.field + idx];
       gg[c] = load_g ? gbuf[(long long)c * g.field + idx] : czero<C>();
+      if (a.ulo) lo[c] = a.ulo[(long long)c * g.field + idx];
     }
-    sweep_mode(in, mx, my, mz, N, phase[mx + my + mz + 3 * N / 2], uu, gg, load_g, rr, a);
+    sweep_mode(in, mx, my, mz, N, phase[mx + my + mz + 3 * N / 2], uu, gg, load_g, rr, a, lo);
     if (a.mode != 0) {
 #pragma unroll
       for (int c = 0; c < 3; ++c) rhs[(long long)c * g.field + idx] = rr[c];
@@ -875,6 +937,7 @@ k_sweep(const C* __restrict__ work, C* __restrict__ u, C* __restrict__ gbuf,
       for (int c = 0; c < 3; ++c) {
         u[(long long)c * g.field + idx] = uu[c];
         gbuf[(long long)c * g.field + idx] = gg[c];
+        if (a.ulo) a.ulo[(long long)c * g.field + idx] = lo[c];
       }
     }
     // The plane mx = N/2 is outside the sphere except at (N/2,0,0): the reference's
@@ -889,6 +952,7 @@ k_sweep(const C* __restrict__ work, C* __restrict__ u, C* __restrict__ gbuf,
         } else {
           u[(long long)c * g.field + inq] = zero;
           gbuf[(long long)c * g.field + inq] = zero;
+          if (a.ulo) a.ulo[(long long)c * g.field + inq] = 0u;
         }
       }
     }
@@ -914,12 +978,14 @@ k_sweep(const C* __restrict__ work, C* __restrict__ u, C* __restrict__ gbuf,
     }
     const long long idx = NH;
     C uu[3], gg[3], rr[3];
+    uint32_t lo[3] = {0u, 0u, 0u};
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       uu[c] = u[(long long)c * g.field + idx];
       gg[c] = load_g ? gbuf[(long long)c * g.field + idx] : czero<C>();
+      if (a.ulo) lo[c] = a.ulo[(long long)c * g.field + idx];
     }
-    sweep_mode(in, NH, 0, 0, N, phase[NH + 3 * N / 2], uu, gg, load_g, rr, a);
+    sweep_mode(in, NH, 0, 0, N, phase[NH + 3 * N / 2], uu, gg, load_g, rr, a, lo);
     if (a.mode != 0) {
 #pragma unroll
       for (int c = 0; c < 3; ++c) rhs[(long long)c * g.field + idx] = rr[c];
@@ -928,6 +994,7 @@ k_sweep(const C* __restrict__ work, C* __restrict__ u, C* __restrict__ gbuf,
       for (int c = 0; c < 3; ++c) {
         u[(long long)c * g.field + idx] = uu[c];
         gbuf[(long long)c * g.field + idx] = gg[c];
+        if (a.ulo) a.ulo[(long long)c * g.field + idx] = lo[c];
       }
     }
   }
@@ -963,12 +1030,14 @@ __global__ void __launch_bounds__(32) k_nyq_mode(C* __restrict__ u, C* __restric
     in.ps[p] = cmk((real_of<C>)part[2 * p + 1], real_of<C>(0));
   }
   C uu[3], gg[3], rr[3];
+  uint32_t lo[3] = {0u, 0u, 0u};
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
     uu[c] = u[(long long)c * g.field + NH];
     gg[c] = load_g ? gbuf[(long long)c * g.field + NH] : czero<C>();
+    if (a.ulo) lo[c] = a.ulo[(long long)c * g.field + NH];
   }
-  sweep_mode(in, NH, 0, 0, N, phase[NH + 3 * N / 2], uu, gg, load_g, rr, a);
+  sweep_mode(in, NH, 0, 0, N, phase[NH + 3 * N / 2], uu, gg, load_g, rr, a, lo);
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
     if (a.mode != 0) {
@@ -976,6 +1045,7 @@ __global__ void __launch_bounds__(32) k_nyq_mode(C* __restrict__ u, C* __restric
     } else {
       u[(long long)c * g.field + NH] = uu[c];
       gbuf[(long long)c * g.field + NH] = gg[c];
+      if (a.ulo) a.ulo[(long long)c * g.field + NH] = lo[c];
     }
   }
 }
@@ -1084,13 +1154,15 @@ k_sweep_rot(const C* __restrict__ work, C* __restrict__ u, C* __restrict__ gbuf,
     const int m2 = mx * mx + my * my + mz * mz;
     const bool keep = 4LL * m2 <= (long long)N * N;
     C r[3], uu[3], gg[3], rr[3];
+    uint32_t lo[3] = {0u, 0u, 0u};
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       r[c] = pair_value(A[c], B[c], ph, keep, a.dealias);
       uu[c] = u[(long long)c * g.field + idx];
       gg[c] = load_g ? gbuf[(long long)c * g.field + idx] : czero<C>();
+      if (a.ulo) lo[c] = a.ulo[(long long)c * g.field + idx];
     }
-    finish_mode(r, mx, my, mz, N, uu, gg, load_g, rr, a);
+    finish_mode(r, mx, my, mz, N, uu, gg, load_g, rr, a, lo);
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       if (a.mode != 0) {
@@ -1098,6 +1170,7 @@ k_sweep_rot(const C* __restrict__ work, C* __restrict__ u, C* __restrict__ gbuf,
       } else {
         u[(long long)c * g.field + idx] = uu[c];
         gbuf[(long long)c * g.field + idx] = gg[c];
+        if (a.ulo) a.ulo[(long long)c * g.field + idx] = lo[c];
       }
     }
   };
@@ -1123,6 +1196,7 @@ k_sweep_rot(const C* __restrict__ work, C* __restrict__ u, C* __restrict__ gbuf,
         } else {
           u[(long long)c * g.field + inq] = czero<C>();
           gbuf[(long long)c * g.field + inq] = czero<C>();
+          if (a.ulo) a.ulo[(long long)c * g.field + inq] = 0u;
         }
       }
     }
@@ -1302,24 +1376,28 @@ k_p5(const __grid_constant__ CUtensorMap map, C* __restrict__ u, C* __restrict__
       // Two-deep software pipeline over this thread's modes: the u, g loads of mode q + 1
       // are in flight while mode q is combined and stored (different modes, no aliasing).
       C uu_n[3], gg_n[3];
-      auto load_mode = [&](int q, C* uu, C* gg) {
+      uint32_t lo_n[3] = {0u, 0u, 0u};
+      auto load_mode = [&](int q, C* uu, C* gg, uint32_t* lo) {
         const long long idx = ((long long)mode_e(q) * N + my) * g.pitch + mx0 + mode_s(q);
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
           uu[c] = u[(long long)c * g.field + idx];
           gg[c] = load_g ? gbuf[(long long)c * g.field + idx] : czero<C>();
+          if (a.ulo) lo[c] = a.ulo[(long long)c * g.field + idx];
         }
       };
-      load_mode(0, uu_n, gg_n);
+      load_mode(0, uu_n, gg_n, lo_n);
 #pragma unroll 1
       for (int q = 0; q < MPT; ++q) {
         C uu[3], gg[3], rr[3];
+        uint32_t lo[3];
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
           uu[c] = uu_n[c];
           gg[c] = gg_n[c];
+          lo[c] = lo_n[c];
         }
-        if (q + 1 < MPT) load_mode(q + 1, uu_n, gg_n);
+        if (q + 1 < MPT) load_mode(q + 1, uu_n, gg_n, lo_n);
         C r3[3];
 #pragma unroll
         for (int c = 0; c < 3; ++c) r3[c] = tmem_ld1<C>(tq + CW * (1 + c) + WPC * q);
@@ -1329,7 +1407,7 @@ k_p5(const __grid_constant__ CUtensorMap map, C* __restrict__ u, C* __restrict__
         const int iz = signed_mode(ez, N);
         const long long row = (long long)ez * N + my;
         const long long idx = row * g.pitch + ix;
-        finish_mode(r3, ix, iy, iz, N, uu, gg, load_g, rr, a);
+        finish_mode(r3, ix, iy, iz, N, uu, gg, load_g, rr, a, lo);
         const bool nyq_zero = ix == 0 && row != 0;  // plane mx = N/2 is zero off (N/2,0,0)
         const long long inq = row * g.pitch + NH;
 #pragma unroll
@@ -1340,9 +1418,11 @@ k_p5(const __grid_constant__ CUtensorMap map, C* __restrict__ u, C* __restrict__
           } else {
             u[(long long)c * g.field + idx] = uu[c];
             gbuf[(long long)c * g.field + idx] = gg[c];
+            if (a.ulo) a.ulo[(long long)c * g.field + idx] = lo[c];
             if (nyq_zero) {
               u[(long long)c * g.field + inq] = czero<C>();
               gbuf[(long long)c * g.field + inq] = czero<C>();
+              if (a.ulo) a.ulo[(long long)c * g.field + inq] = 0u;
             }
           }
         }
@@ -1527,7 +1607,16 @@ __device__ __forceinline__ double2 widen(double2 v) { return v; }
 __device__ __forceinline__ double2 widen(float2 v) { return make_double2(v.x, v.y); }
 
 template <class C>
-__global__ void k_half_to_full(const C* __restrict__ half, double2* __restrict__ full, Geom g) {
+__device__ __forceinline__ double2 widen_comp(const C* half, const uint32_t* lo, long long i) {
+  if constexpr (sizeof(C) == 8) {
+    if (lo) return comp_decode(half[i], lo[i]);
+  }
+  return widen(half[i]);
+}
+
+template <class C>
+__global__ void k_half_to_full(const C* __restrict__ half, double2* __restrict__ full, Geom g,
+                               const uint32_t* __restrict__ lo) {
   const long long n = g.n;
   const long long total = n * n * n;
   const long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -1535,10 +1624,10 @@ __global__ void k_half_to_full(const C* __restrict__ half, double2* __restrict__
   const int x = (int)(id % n);
   const long long y = (id / n) % n, z = id / (n * n);
   if (x <= g.nh) {
-    full[id] = widen(half[(z * n + y) * g.pitch + x]);
+    full[id] = widen_comp(half, lo, (z * n + y) * g.pitch + x);
   } else {
     const long long ym = (n - y) % n, zm = (n - z) % n;
-    full[id] = widen(cconj(half[(zm * n + ym) * g.pitch + (n - x)]));
+    full[id] = cconj(widen_comp(half, lo, (zm * n + ym) * g.pitch + (n - x)));
   }
 }
 
@@ -1546,7 +1635,7 @@ __global__ void k_half_to_full(const C* __restrict__ half, double2* __restrict__
 // (c_m + conj(c_-m))/2 is stored, so a c2r of the result equals Re(IDFT(c)).
 template <class C>
 __global__ void k_full_to_half(const double2* __restrict__ full, C* __restrict__ half, int hermitian_part,
-                               Geom g) {
+                               Geom g, uint32_t* __restrict__ lo) {
   const long long n = g.n;
   const long long total = n * n * (g.nh + 1);
   const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -1559,6 +1648,12 @@ __global__ void k_full_to_half(const double2* __restrict__ full, C* __restrict__
     const long long ym = (n - y) % n, zm = (n - z) % n, xm = (n - x) % n;
     const double2 w = full[(zm * n + ym) * n + xm];
     v = make_double2(0.5 * (v.x + w.x), 0.5 * (v.y - w.y));
+  }
+  if constexpr (sizeof(C) == 8) {
+    if (lo) {  // FP32 form, compensated: the remainder the FP32 value drops goes to lo
+      half[row * g.pitch + x] = comp_encode(v, &lo[row * g.pitch + x]);
+      return;
+    }
   }
   using RT = real_of<C>;
   half[row * g.pitch + x] = cmk((RT)v.x, (RT)v.y);
@@ -1909,17 +2004,21 @@ void launch_add_sparse(void* u, int precision, const long long* idx, const doubl
   if (precision == 0) k_add_sparse<double2><<<blocks_for(count, 256), 256, 0, st>>>(FC<double2>(u), idx, val, count);
   else k_add_sparse<float2><<<blocks_for(count, 256), 256, 0, st>>>(FC<float2>(u), idx, val, count);
 }
-void launch_half_to_full(const void* half, int precision, double2* full, Geom g, cudaStream_t st) {
+void launch_half_to_full(const void* half, int precision, double2* full, Geom g, cudaStream_t st,
+                         const uint32_t* lo) {
   const long long total = (long long)g.n * g.n * g.n;
-  if (precision == 0) k_half_to_full<double2><<<blocks_for(total, 256), 256, 0, st>>>(FC<double2>(half), full, g);
-  else k_half_to_full<float2><<<blocks_for(total, 256), 256, 0, st>>>(FC<float2>(half), full, g);
+  if (precision == 0)
+    k_half_to_full<double2><<<blocks_for(total, 256), 256, 0, st>>>(FC<double2>(half), full, g, nullptr);
+  else k_half_to_full<float2><<<blocks_for(total, 256), 256, 0, st>>>(FC<float2>(half), full, g, lo);
 }
 void launch_full_to_half(const double2* full, void* half, int precision, int hermitian_part, Geom g,
-                         cudaStream_t st) {
+                         cudaStream_t st, uint32_t* lo) {
   const long long total = (long long)g.n * g.n * (g.nh + 1);
   if (precision == 0)
-    k_full_to_half<double2><<<blocks_for(total, 256), 256, 0, st>>>(full, FC<double2>(half), hermitian_part, g);
-  else k_full_to_half<float2><<<blocks_for(total, 256), 256, 0, st>>>(full, FC<float2>(half), hermitian_part, g);
+    k_full_to_half<double2><<<blocks_for(total, 256), 256, 0, st>>>(full, FC<double2>(half), hermitian_part, g,
+                                                                      nullptr);
+  else
+    k_full_to_half<float2><<<blocks_for(total, 256), 256, 0, st>>>(full, FC<float2>(half), hermitian_part, g, lo);
 }
 void launch_spectral_diag(const void* u, int precision, double* partials, int nblocks, Geom g, cudaStream_t st) {
   if (precision == 0) k_spectral_diag<double2><<<nblocks, 256, 0, st>>>(FC<double2>(u), partials, g);

@@ -37,6 +37,10 @@ struct SweepArgs {
   int mode;        // 0: RK update of (u, g); 1: projected RHS to `rhs`; 2: masked nonlinear term only
   int dealias;     // 1: phase-shift pair, 0: plain product only
   int visc_if;     // 0: explicit viscous term in the RHS (the reference); 1: integrating factor
+  // FP32 precision form, compensated state: one word per complex value of u (same index as
+  // u; a bf16 pair, re in the low half) holding the part of the FP64 update that the FP32
+  // value cannot; null: u is the FP32 value alone (and always in the FP64 form)
+  uint32_t* ulo;
 };
 
 // Arguments of the TMA-fed streaming y/z pass.
@@ -114,9 +118,12 @@ void launch_project_truncate(void* u, int precision, Geom g, cudaStream_t st);
 void launch_add_sparse(void* u, int precision, const long long* idx, const double2* val, int count,
                        cudaStream_t st);
 // half field <-> the reference's full layout (always complex doubles on that side)
-void launch_half_to_full(const void* half, int precision, double2* full, Geom g, cudaStream_t st);
+// `lo` (FP32 form, may be null): the compensation words of the half field (see SweepArgs::ulo);
+// half_to_full adds them, full_to_half writes the remainder the FP32 value drops
+void launch_half_to_full(const void* half, int precision, double2* full, Geom g, cudaStream_t st,
+                         const uint32_t* lo = nullptr);
 void launch_full_to_half(const double2* full, void* half, int precision, int hermitian_part, Geom g,
-                         cudaStream_t st);
+                         cudaStream_t st, uint32_t* lo = nullptr);
 void launch_spectral_diag(const void* u, int precision, double* partials, int nblocks, Geom g, cudaStream_t st);
 void launch_reduce(const double* partials, int count, int stride, int op_max, double* out, cudaStream_t st);
 

@@ -15,8 +15,10 @@
 //     contents; each call clears its work region before use.  Calls whose GPU work
 //     overlaps (other host threads, or other streams) race on it;
 //   * the first call on a device does the set-up (symbol address, twiddle upload,
-//     kernel attributes) with that device current; make that first call before any
-//     stream capture begins.
+//     kernel attributes) with that device current;
+//   * every call returns only after its work on the stream finished (it synchronises the
+//     stream), so a call on a stream that is being captured is refused with
+//     SNS_ERR_INVALID before anything is enqueued.
 #include "sns_kernels.cuh"
 #include "../../include/sns_b200.h"
 
@@ -105,15 +107,19 @@ int setup_device(int dev, double2** base) {
 
 using GetAddressRange = PFN_cuMemGetAddressRange_v3020;
 
+// The driver's cuMemGetAddressRange, looked up once (a function-local static: its
+// initialisation is thread-safe); null when the driver does not export it.
 GetAddressRange address_range_fn() {
-  static GetAddressRange fn = nullptr;
-  if (fn == nullptr) {
+  static const GetAddressRange fn = [] {
     void* p = nullptr;
     cudaDriverEntryPointQueryResult q{};
-    if (cudaGetDriverEntryPoint("cuMemGetAddressRange", &p, cudaEnableDefault, &q) == cudaSuccess &&
-        q == cudaDriverEntryPointSuccess)
-      fn = reinterpret_cast<GetAddressRange>(p);
-  }
+    if (cudaGetDriverEntryPoint("cuMemGetAddressRange", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess) {
+      cudaGetLastError();
+      return GetAddressRange(nullptr);
+    }
+    return reinterpret_cast<GetAddressRange>(p);
+  }();
   return fn;
 }
 
@@ -136,19 +142,21 @@ int check_device_buffer(const void* ptr, size_t bytes, size_t align, int dev, co
     std::snprintf(buf, sizeof buf, "%s: must be device memory of the current device %d", name, dev);
     return fail(SNS_ERR_INVALID, buf);
   }
+  // without the size check the kernels could write past the caller's allocation: refuse
   GetAddressRange range = address_range_fn();
-  if (range != nullptr) {
-    CUdeviceptr base = 0;
-    size_t size = 0;
-    if (range(&base, &size, (CUdeviceptr)ptr) != CUDA_SUCCESS) {
-      std::snprintf(buf, sizeof buf, "%s: cuMemGetAddressRange failed", name);
-      return fail(SNS_ERR_INVALID, buf);
-    }
-    if ((CUdeviceptr)ptr + bytes > base + size) {
-      std::snprintf(buf, sizeof buf, "%s: allocation holds %zu bytes from this pointer, %zu needed", name,
-                    (size_t)(base + size - (CUdeviceptr)ptr), bytes);
-      return fail(SNS_ERR_INVALID, buf);
-    }
+  if (range == nullptr)
+    return fail(SNS_ERR_UNSUPPORTED, "cuMemGetAddressRange is not available from the driver: buffer sizes "
+                                     "cannot be checked");
+  CUdeviceptr base = 0;
+  size_t size = 0;
+  if (range(&base, &size, (CUdeviceptr)ptr) != CUDA_SUCCESS) {
+    std::snprintf(buf, sizeof buf, "%s: cuMemGetAddressRange failed", name);
+    return fail(SNS_ERR_INVALID, buf);
+  }
+  if ((CUdeviceptr)ptr + bytes > base + size) {
+    std::snprintf(buf, sizeof buf, "%s: allocation holds %zu bytes from this pointer, %zu needed", name,
+                  (size_t)(base + size - (CUdeviceptr)ptr), bytes);
+    return fail(SNS_ERR_INVALID, buf);
   }
   return SNS_OK;
 }
@@ -174,6 +182,23 @@ extern "C" int sns_forward_r2c_noalloc(int n, const double* dev_physical, double
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return fail_cuda("cudaGetDevice", e);
   if (dev < 0 || dev >= kMaxDevices) return fail(SNS_ERR_UNSUPPORTED, "device ordinal beyond the static slots");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  {
+    // the call ends with a stream synchronisation, which a capturing stream cannot take
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    e = cudaStreamIsCapturing(st, &cs);
+    if (e != cudaSuccess) return fail_cuda("sns_forward_r2c_noalloc: stream", e);
+    if (cs != cudaStreamCaptureStatusNone)
+      return fail(SNS_ERR_INVALID, "sns_forward_r2c_noalloc: the stream is being captured; the call synchronises "
+                                   "its stream and cannot be recorded into a graph");
+    // a caller's stream must belong to the current device, like the buffers
+    if (st != nullptr) {
+      int sdev = -1;
+      e = cudaStreamGetDevice(st, &sdev);
+      if (e != cudaSuccess) return fail_cuda("sns_forward_r2c_noalloc: stream", e);
+      if (sdev != dev) return fail(SNS_ERR_INVALID, "sns_forward_r2c_noalloc: the stream belongs to another device");
+    }
+  }
   const size_t np = (size_t)n * n * n;
   int rc = check_device_buffer(dev_physical, np * sizeof(double), sizeof(double), dev, "dev_physical");
   if (rc != SNS_OK) return rc;
@@ -185,7 +210,6 @@ extern "C" int sns_forward_r2c_noalloc(int n, const double* dev_physical, double
 
   const sns::Ops* ops = sns::ops_for(n);
   const sns::Geom g{n, n / 2, sns::pitch_for(n), (long long)n * n * sns::pitch_for(n)};
-  cudaStream_t st = static_cast<cudaStream_t>(stream);
   double2* work = base;
   const double2* tw = base + kFieldElems + twiddle_offset(n);
   const int tiles = g.pitch / 8;  // Nyquist column and padding included, as sns_forward_r2c

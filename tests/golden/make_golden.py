@@ -46,7 +46,9 @@ def parse(path):
 
 
 def main():
-    src = sys.argv[1] if len(sys.argv) > 1 else "/root/reference/Benchmark.md"
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py <path to the reference's Benchmark.md>")
+    src = sys.argv[1]
     data = {"what": "FP64 t = 20 finals of the reference's adaptive-CFL Taylor-Green benchmark "
                     "(CFL 0.5, dt cap 0.5, t_end 20, output_dt 1)", "runs": parse(src)}
     dst = os.path.join(os.path.dirname(os.path.abspath(__file__)), "benchmark_finals.json")

@@ -4,10 +4,11 @@ from their own pool, runs near the HBM limit, loops that cannot take the synchro
 an allocation may cause).  Its scratch is a fixed __device__ array inside the library, so
 it serves grids up to N = 64 only.
 
-The GPU test calls it through the C ABI on device buffers and checks it against the
-handle-based sns_forward_r2c, on two calls in a row (the second reuses the shared scratch
-that the first one left behind), to the FFT tolerance of the other GPU tests: max abs
-error <= 1e-12 * max|X|.  This file is collected last on purpose.
+The GPU tests call it through the C ABI on device buffers and check it against the
+handle-based sns_forward_r2c and against numpy's fftn, on two calls in a row (the second
+reuses the shared scratch that the first one left behind), to the FFT tolerance of the other
+GPU tests: max abs error <= 1e-12 * max|X|; and once more on a caller's own non-default
+stream.  This file is collected last on purpose.
 """
 import ctypes as C
 
@@ -50,6 +51,33 @@ def test_noalloc_forward_matches_handle_forward(lib):
         assert rc == _lib.SNS_OK, lib.sns_last_error(None)
         got = d_out.cpu().numpy().view(np.complex128).reshape(n, n, n)
         assert np.max(np.abs(got - want)) <= TOL * np.max(np.abs(want)), n
+        # and directly against numpy (x fastest: the array is indexed [iz, iy, ix])
+        ref = np.fft.fftn(x)
+        assert np.max(np.abs(got - ref)) <= TOL * np.max(np.abs(ref)), n
+
+
+@pytest.mark.gpu
+def test_noalloc_forward_on_callers_stream(lib):
+    """The documented use on a stream the caller owns: the call enqueues its work there and
+    returns after that stream finished."""
+    import torch
+
+    dev = torch.device("cuda:0")
+    torch.cuda.set_device(dev)
+    rng = np.random.default_rng(7)
+    n = 48
+    x = rng.standard_normal((n, n, n))
+    side = torch.cuda.Stream(device=dev)
+    d_in = torch.from_numpy(x).to(dev)
+    d_out = torch.full((2 * n ** 3,), float("nan"), dtype=torch.float64, device=dev)
+    torch.cuda.synchronize()
+    for _ in range(2):
+        rc = lib.sns_forward_r2c_noalloc(n, C.c_void_p(d_in.data_ptr()), C.c_void_p(d_out.data_ptr()),
+                                         C.c_void_p(side.cuda_stream))
+        assert rc == _lib.SNS_OK, lib.sns_last_error(None)
+        got = d_out.cpu().numpy().view(np.complex128).reshape(n, n, n)
+        ref = np.fft.fftn(x)
+        assert np.max(np.abs(got - ref)) <= TOL * np.max(np.abs(ref))
 
 
 @pytest.mark.gpu
