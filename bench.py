@@ -193,23 +193,32 @@ def max_over_ranks(pg, value: float) -> float:
     return float(t.item())
 
 
-def cpu_oracle_rate(n: int, sample_stages: int = 1):
-    """Time the CPU oracle (half-spectrum restatement, scipy pocketfft with every host
-    thread) on `sample_stages` RK3 stages at N^3; returns (Gpt*steps/s, seconds, threads)."""
-    from oracle import ref_r2c
-    threads = os.cpu_count() or 1
-    s = ref_r2c.TaylorGreenR2C(n, RE, workers=threads)
-    s.g = [None, None, None]
-    t0 = time.perf_counter()
-    for _ in range(sample_stages):
-        r = s.compute_rhs()
-        for c in range(3):
-            s.g[c] = r[c]
-            s.u_hat[c] = s.u_hat[c] + s.g[c] * (DT / 3.0)
-        s.project_truncate(s.u_hat)
-    dt = time.perf_counter() - t0
-    steps = sample_stages / 3.0
-    return n ** 3 * steps / dt / 1e9, dt, threads
+class OracleStages:
+    """The CPU oracle (oracle/ref_r2c.py: scipy pocketfft and the element-wise work on every
+    host thread) advanced one RK3 stage per sample: stages 0, 1, 2, 0, ... with the Williamson
+    coefficients, so three consecutive samples are one whole RK3 step (g carried between
+    them).  A sample is N^3 / 3 grid-point * RK3-steps of work."""
+
+    def __init__(self, n: int, precision: str):
+        from oracle import ref_r2c
+        self.threads = os.cpu_count() or 1
+        self.n = n
+        self.s = ref_r2c.TaylorGreenR2C(n, RE, workers=self.threads, precision=precision)
+        self.k = 0
+
+    def sample(self) -> float:
+        t0 = time.perf_counter()
+        self.s.stage(DT, self.k % 3)
+        self.k += 1
+        return time.perf_counter() - t0
+
+
+def cpu_oracle_rate(n: int, precision: str = "fp64", samples: int = 1):
+    """Gpt*RK3-steps/s of the CPU oracle over `samples` consecutive stages at N^3; returns
+    (rate, seconds, threads)."""
+    o = OracleStages(n, precision)
+    secs = sum(o.sample() for _ in range(samples))
+    return n ** 3 * (samples / 3.0) / secs / 1e9, secs, o.threads
 
 
 def cpu_model() -> str:
@@ -237,37 +246,68 @@ def cpu_oracle_config1(steps: int = 40):
     return 64 ** 3 * steps / dt, dt, threads
 
 
+def workload_config(n: int, head: str, world: int) -> dict:
+    """The `config` of the JSON line, the same for both arms (the reference arm runs the
+    same workload on the host cores)."""
+    cb = 16 if head == "fp64" else 8
+    pitch = ((n // 2 + 1) + 128 // cb - 1) // (128 // cb) * (128 // cb)
+    # 18 half fields, plus the FP32 form's compensation words of u (3 fields of 4 B per value)
+    resident = (18 * n * n * pitch * cb + (3 * n * n * pitch * 4 if head == "fp32" else 0)) / 1e9
+    return {"workload": f"Taylor-Green RK3 step, {n}^3, "
+                        + ("FP32 precision form (mixed)" if head == "fp32" else "FP64 plain drop-in form")
+                        + " (phase-shift dealiasing, sphere truncation, explicit viscosity)",
+            "n": n, "precision": head, "reynolds": RE, "dt": DT,
+            "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
+            "l2": f"inputs larger than L2 ({resident:.1f} GB resident)"}
+
+
 def run_reference(args, world, rank, pg):
-    """--impl reference: the reference's CPU path on the host cores.  The reference itself
-    cannot be built here (FFTW3, MPI, AVA and FLUPS are absent), so its CPU restatement
-    (the oracle) is what runs."""
+    """--impl reference: the reference's CPU path on the host cores, on this arm's workload.
+    The reference itself cannot be built here (FFTW3, MPI, AVA and FLUPS are absent), so its
+    CPU restatement (the oracle) runs, with every host thread, in the headline's precision
+    (the reference's single-precision build for the FP32 form).  Each timed "step" is one
+    sample: one RK3 stage at N^3 (a third of an RK3 step, stages cycling 0, 1, 2), since a
+    whole 512^3 step takes the CPU tens of seconds; `value` counts N^3 / 3 grid-point *
+    RK3-steps per sample, and steps * ms_per_step is the timed region.  One FP64 stage is
+    timed after the region for the like-for-like ratio of the FP64 drop-in."""
     if rank != 0:
         return 0
     n = args.n
-    # warm-up: the code paths and pocketfft plans on a small grid (a 512^3 stage is ~30 s)
-    for _ in range(max(1, min(args.warmup, 3))):
-        cpu_oracle_rate(64, 1)
-    # each timed "step" is one RK3 stage at N^3; capped so the arm ends within minutes
-    k = max(1, min(args.steps, 4 if n >= 512 else args.steps))
-    total_s = 0.0
+    head = "fp32" if args.precision in ("both", "fp32") else "fp64"
+    o = OracleStages(n, head)
+    # warm-up (untimed): one stage at N^3 (pocketfft plans, page-in), the rest at 64^3
+    for i in range(args.warmup):
+        if i == 0:
+            o.sample()
+        else:
+            cpu_oracle_rate(64, head, 1)
+    o.k = 0
+    secs = [o.sample() for _ in range(args.steps)]
+    total_s = sum(secs)
+    value = n ** 3 * (args.steps / 3.0) / total_s / 1e9
+    del o
+    r64 = s64 = None
+    if head == "fp32":
+        r64, s64, _ = cpu_oracle_rate(n, "fp64", 1)
     threads = os.cpu_count() or 1
-    for _ in range(k):
-        _, s, threads = cpu_oracle_rate(n, 1)
-        total_s += s
-    units = n ** 3 * (k / 3.0)
-    value = units / total_s / 1e9
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
-        "steps": k, "warmup": args.warmup, "ms_per_step": 3 * 1e3 * total_s / k,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic: analytic Taylor-Green initial field",
-        "config": {"workload": f"Taylor-Green RK3, {n}^3, FP64 plain, Re=1600, dt=1e-3", "n": n,
-                   "precision": "fp64", "each_step": "one RK3 stage (1/3 step) of the CPU oracle"},
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total_s / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32" if head == "fp32" else "f64",
+        "data": "synthetic: analytic Taylor-Green initial field (Re=1600)",
+        "config": workload_config(n, head, world),
+        "each_step": f"one RK3 stage at {n}^3 (stages 0, 1, 2 in turn: three samples are one RK3 step)",
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
-                         "sample": f"{k} RK3 stages at {n}^3 (oracle/ref_r2c.py, scipy pocketfft, "
-                                   f"{threads} threads); reference FFTW path unbuildable here"},
+                         "sample": f"{args.steps} consecutive RK3 stages at {n}^3 of the CPU oracle "
+                                   f"(oracle/ref_r2c.py, {head}, scipy pocketfft and element-wise work on "
+                                   f"{threads} threads); the reference's FFTW path cannot be built here",
+                         "cpu_model": cpu_model()},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    if r64 is not None:
+        line["fp64_stage"] = {"value": r64, "unit": UNIT, "seconds": s64,
+                              "what": f"one FP64 RK3 stage at {n}^3 (the FP64 drop-in's CPU counterpart)"}
     print(json.dumps(line), flush=True)
     return 0
 
@@ -371,30 +411,28 @@ def run_b200(args, world, rank, local, pg):
     if rank == 0:
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
-            rate, secs, threads = cpu_oracle_rate(n, 1)
+            # the CPU oracle in the headline's precision (3 stages = one RK3 step at N^3), and
+            # one FP64 stage for the FP64 drop-in's like-for-like ratio
+            rate, secs, threads = cpu_oracle_rate(n, head, 3)
+            rate64, secs64, _ = cpu_oracle_rate(n, "fp64", 1) if head != "fp64" else (rate, secs, threads)
             r64, s64, _ = cpu_oracle_config1()
             cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
-                   "sample": f"1 RK3 stage at {n}^3 ({secs:.1f} s) of the CPU oracle (oracle/ref_r2c.py, scipy "
-                             f"pocketfft, {threads} threads, FP64); the reference's FFTW path cannot be built here",
+                   "sample": f"one RK3 step (3 stages) at {n}^3 ({secs:.1f} s) of the CPU oracle (oracle/ref_r2c.py, "
+                             f"{head}, scipy pocketfft and element-wise work on {threads} threads); the reference's "
+                             f"FFTW path cannot be built here",
                    "cpu_model": cpu_model(),
+                   "fp64": {"value": rate64, "unit": UNIT, "sample": f"1 FP64 RK3 stage at {n}^3 ({secs64:.1f} s)"},
                    "config1_64": {"value": r64 / 1e9, "unit": UNIT, "gpt_steps_per_s": r64,
                                   "sample": f"40 RK3 steps at 64^3, dt 5e-3 ({s64:.1f} s, {threads} threads)",
                                   "reference_published_gpt_steps_per_s": [1.39e6, 2.47e6]}}
         r = results[head]
-        cb = 16 if head == "fp64" else 8
-        resident = 18 * n * n * (((n // 2 + 1) + 128 // cb - 1) // (128 // cb) * (128 // cb)) * cb / 1e9
         line = {
             "metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": r["ms_per_step"], "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None,
             "dtype": "f32 (FP64 twiddles, IF exponent and reductions)" if head == "fp32" else "f64",
             "data": "synthetic: analytic Taylor-Green initial field (Re=1600)",
-            "config": {"workload": f"Taylor-Green RK3 step, {n}^3, "
-                                   + ("FP32 precision form (mixed)" if head == "fp32" else "FP64 plain drop-in form")
-                                   + " (phase-shift dealiasing, sphere truncation, explicit viscosity)",
-                       "n": n, "precision": head, "reynolds": RE, "dt": DT,
-                       "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
-                       "l2": f"inputs larger than L2 ({resident:.1f} GB resident)"},
+            "config": workload_config(n, head, world),
             "clocks": r["clocks"],
             "gpu_launches": LAUNCHES_PER_STEP * args.steps,
             "roofline": r["roofline"],
@@ -419,6 +457,11 @@ def run_b200(args, world, rank, local, pg):
                 "rel_enstrophy": abs(d32["enstrophy"] - d64["enstrophy"]) / d64["enstrophy"]}
         if cpu is not None:
             line["cpu_baseline"] = cpu
+            if "fp64_plain" in line:
+                # like for like: the FP64 drop-in over the FP64 CPU oracle, the FP32 form over
+                # the FP32 one
+                line["fp64_plain"]["vs_cpu_fp64"] = line["fp64_plain"]["value"] / cpu["fp64"]["value"]
+            line["vs_cpu_same_precision"] = r["value"] / cpu["value"]
         extra = run_multi(args) if world == 1 else {}
         line.update(extra)
         print(json.dumps(line), flush=True)

@@ -24,6 +24,7 @@ Arrays are indexed ``[iz, iy, mx]`` (x fastest, as the reference layout).
 from __future__ import annotations
 
 import os
+from concurrent.futures import ThreadPoolExecutor
 
 import numpy as np
 import scipy.fft as sfft
@@ -62,31 +63,54 @@ class TaylorGreenR2C:
     """Half-spectrum restatement of ``TaylorGreenSolver::Impl`` with identical numerics."""
 
     def __init__(self, n: int, reynolds: float, u_hat0=None, workers: int | None = None,
-                 integrating_factor: bool = False, rotational: bool = False):
+                 integrating_factor: bool = False, rotational: bool = False, precision: str = "fp64"):
+        """precision "fp32" runs the same arithmetic on complex64/float32 arrays, as the
+        reference's single-precision build does (``Real = float``,
+        ``ava_taylor_green_impl.hpp:48-51``); it times the CPU path of the FP32 form and is
+        not a parity reference."""
         if n <= 0:
             raise ValueError("grid size must be positive")
         if reynolds <= 0.0:
             raise ValueError("Reynolds number must be positive")
+        if precision not in ("fp64", "fp32"):
+            raise ValueError("precision must be fp64 or fp32")
         self.n = n
         self.nu = 1.0 / reynolds
         self.integrating_factor = integrating_factor
         self.rotational = rotational
         self.global_size = n * n * n
         self.workers = WORKERS if workers is None else workers
+        self.precision = precision
+        self.rdtype = np.float64 if precision == "fp64" else np.float32
+        self.cdtype = np.complex128 if precision == "fp64" else np.complex64
+        self._pool = None
         mx, my, mz = half_mode_grids(n)
         msum = (mx + my + mz).astype(np.float64)
         angle = (msum * PI) / float(n)  # initialize_metadata :782-783
-        self.phase = np.cos(angle) + 1j * np.sin(angle)
+        self.phase = (np.cos(angle) + 1j * np.sin(angle)).astype(self.cdtype)
         h = 0.5 * float(n)
         m2 = (mx * mx + my * my + mz * mz).astype(np.float64)
         self.keep = (m2 / (h * h)) <= 1.0  # keep_mode_host :131-134
-        self.k2 = m2
-        self.kvals = (mx.astype(np.float64), my.astype(np.float64), mz.astype(np.float64))
+        self.k2 = m2.astype(self.rdtype)
+        self.kvals = tuple(k.astype(self.rdtype) for k in (mx, my, mz))
         self.g = [None, None, None]
         if u_hat0 is None:
             self.initialize_velocity()
         else:
-            self.u_hat = [np.array(c, np.complex128, copy=True) for c in u_hat0]
+            self.u_hat = [np.array(c, self.cdtype, copy=True) for c in u_hat0]
+
+    def _slabs(self, fn):
+        """Run fn(s) over z-slabs s that cover axis 0, on the worker threads (numpy releases
+        the GIL inside its loops).  Every element is computed by the same expression whatever
+        the split, so the results do not depend on the thread count."""
+        k = max(1, min(self.workers, self.n))
+        if k == 1:
+            fn(slice(None))
+            return
+        if self._pool is None:
+            self._pool = ThreadPoolExecutor(k)
+        b = np.linspace(0, self.n, k + 1).astype(int)
+        list(self._pool.map(fn, [slice(b[i], b[i + 1]) for i in range(k)]))
 
     def forward(self, phys):
         return sfft.rfftn(phys, workers=self.workers)
@@ -103,7 +127,7 @@ class TaylorGreenR2C:
         p0 = np.broadcast_to(np.sin(x) * np.cos(y) * np.cos(z), (n,) * 3)
         p1 = np.broadcast_to(-np.cos(x) * np.sin(y) * np.cos(z), (n,) * 3)
         p2 = np.zeros((n, n, n))
-        self.u_hat = [self.forward(np.ascontiguousarray(p)) for p in (p0, p1, p2)]
+        self.u_hat = [self.forward(np.ascontiguousarray(p, dtype=self.rdtype)) for p in (p0, p1, p2)]
         self.project_truncate(self.u_hat)
 
     def project_truncate(self, f):
@@ -118,20 +142,36 @@ class TaylorGreenR2C:
         f[2][...] = np.where(ok, f[2] - factor * iz, 0.0)
 
     def nonlinear(self, u_hat):
-        """Masked conservative-form nonlinear term only (before viscosity and projection)."""
+        """Masked conservative-form nonlinear term only (before viscosity and projection).
+        The element-wise work runs on z-slabs in the worker threads (``_slabs``); per element
+        it is the reference's expression: value = (c0 + cs conj(phase)) / 2, masked, then
+        r_a -= i k_b value and r_b -= i k_a value (:926-936)."""
         phys = [self.backward_real(u) for u in u_hat]
         shift = [self.backward_real(u * self.phase) for u in u_hat]
         rhs = [np.zeros_like(u_hat[0]) for _ in range(3)]
-        kv = self.kvals
-        cphase = np.conj(self.phase)
+        shape = rhs[0].shape
+        keep = np.broadcast_to(self.keep, shape)
+        kvb = [np.broadcast_to(k, shape) for k in self.kvals]
+        ph = np.broadcast_to(np.conj(self.phase), shape)
+        p = np.empty_like(phys[0])
         for a, b in ((0, 0), (0, 1), (0, 2), (1, 1), (1, 2), (2, 2)):
-            c0 = self.forward(phys[a] * phys[b])
-            cs = self.forward(shift[a] * shift[b])
-            value = 0.5 * (c0 + cs * cphase)
-            value = np.where(self.keep, value, 0.0)
-            rhs[a] = rhs[a] + (-1j) * kv[b] * value
-            if a != b:
-                rhs[b] = rhs[b] + (-1j) * kv[a] * value
+            def mul0(s):
+                np.multiply(phys[a][s], phys[b][s], out=p[s])
+            self._slabs(mul0)
+            c0 = self.forward(p)
+
+            def muls(s):
+                np.multiply(shift[a][s], shift[b][s], out=p[s])
+            self._slabs(muls)
+            cs = self.forward(p)
+
+            def combine(s):
+                value = 0.5 * (c0[s] + cs[s] * ph[s])
+                value = np.where(keep[s], value, 0.0)
+                rhs[a][s] = rhs[a][s] + (-1j) * kvb[b][s] * value
+                if a != b:
+                    rhs[b][s] = rhs[b][s] + (-1j) * kvb[a][s] * value
+            self._slabs(combine)
         return rhs
 
     def nonlinear_rotational(self, u_hat):
@@ -174,26 +214,31 @@ class TaylorGreenR2C:
                 u[c] = u[c] * f
                 g[c] = g[c] * f
 
-    def step(self, dt: float):
+    def stage(self, dt: float, s: int):
+        """Stage s (0, 1, 2) of the Williamson low-storage RK3 step (``Impl::step``,
+        ``ava_taylor_green_impl.hpp:979-1045``): g = a_s g + H(u); u += b_s dt g; P(u)."""
         u, g = self.u_hat, self.g
         r = self.compute_rhs()
-        for c in range(3):
-            g[c] = r[c].copy()
-            u[c] = u[c] + g[c] * (dt / 3.0)
-        self._if_advance(u, g, dt / 3.0)
+        if s == 0:
+            for c in range(3):
+                g[c] = r[c].copy()
+                u[c] = u[c] + g[c] * (dt / 3.0)
+            self._if_advance(u, g, dt / 3.0)
+        elif s == 1:
+            for c in range(3):
+                g[c] = g[c] * (-5.0 / 9.0) + r[c]
+                u[c] = u[c] + g[c] * (15.0 * dt / 16.0)
+            self._if_advance(u, g, 5.0 * dt / 12.0)
+        else:
+            for c in range(3):
+                g[c] = g[c] * (-153.0 / 128.0) + r[c]
+                u[c] = u[c] + g[c] * (8.0 * dt / 15.0)
+            self._if_advance(u, g, dt / 4.0)
         self.project_truncate(u)
-        r = self.compute_rhs()
-        for c in range(3):
-            g[c] = g[c] * (-5.0 / 9.0) + r[c]
-            u[c] = u[c] + g[c] * (15.0 * dt / 16.0)
-        self._if_advance(u, g, 5.0 * dt / 12.0)
-        self.project_truncate(u)
-        r = self.compute_rhs()
-        for c in range(3):
-            g[c] = g[c] * (-153.0 / 128.0) + r[c]
-            u[c] = u[c] + g[c] * (8.0 * dt / 15.0)
-        self._if_advance(u, g, dt / 4.0)
-        self.project_truncate(u)
+
+    def step(self, dt: float):
+        for s in range(3):
+            self.stage(dt, s)
 
     step_rk3 = step
 

@@ -453,6 +453,21 @@ struct XP {
 
 __device__ __forceinline__ int pp16(int e) { return e + (e >> 4); }
 
+// W_32^q = exp(-2*pi*i*q/32), q < 16, as the twiddle table holds it (exp(-2*pi*i*t/512) at
+// t = 16 q, rounded from long double; the FP32 form rounds these doubles), so the radix-32
+// combine of the two-stage x pass multiplies by immediates instead of loading them.
+__host__ __device__ constexpr double w32_cos(int q) {  // cos(pi q / 16), 0 <= q <= 8
+  return q == 0 ? 1.0 : q == 1 ? 0.98078528040323043 : q == 2 ? 0.92387953251128674 : q == 3 ? 0.83146961230254524
+       : q == 4 ? 0.70710678118654757 : q == 5 ? 0.55557023301960218 : q == 6 ? 0.38268343236508978
+       : q == 7 ? 0.19509032201612828 : 0.0;
+}
+template <class C>
+__device__ __forceinline__ C w32(int q) {  // 0 <= q < 16 (unrolled: folds to immediates)
+  const double re = q <= 8 ? w32_cos(q) : -w32_cos(16 - q);
+  const double im = q <= 8 ? -w32_cos(8 - q) : -w32_cos(q - 8);
+  return cmk((real_of<C>)re, (real_of<C>)im);
+}
+
 template <class C>
 __device__ __forceinline__ C shfl2(C v, int src) {
   return cmk(__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src));
@@ -499,6 +514,27 @@ k_xpass2(C* __restrict__ work, const C* __restrict__ unyq, const C* __restrict__
     }
   };
   if (tid == 0 && blockIdx.x < niter) issue(blockIdx.x, 0);
+  // Stage-B twiddles W_N^(j*rr), rr = 2 i + h: the same for every row this thread transforms
+  // (inverse and forward stages B share the lane mapping).  In the FP32 form with the radix-32
+  // split they come from 8 values held in registers, W^(j (h + 2 c)) * W^(8 j a) with
+  // i = 4 a + c, instead of 16 shared-memory loads per FFT (the x pass is bound by its
+  // shared-memory pipe); the FP64 form has no registers to spare and loads them.
+  constexpr bool kTwReg = X::PAIR && sizeof(C) == 8;
+  C twP[4], twQ[4];
+  if constexpr (kTwReg) {
+    const int j = tid & 15, h = (tid >> 4) & 1;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) twP[c] = tw2[(h + 2 * c) * 16 + j];
+#pragma unroll
+    for (int a = 0; a < 4; ++a) twQ[a] = tw2[8 * a * 16 + j];
+  }
+  auto stage_b_tw = [&](int i, int j, int h) -> C {
+    if constexpr (kTwReg) {
+      return i < 4 ? twP[i] : cmul(twP[i & 3], twQ[i >> 2]);
+    } else {
+      return tw2[(2 * i + h) * 16 + j];
+    }
+  };
   double nyq_p0 = 0.0, nyq_ps = 0.0;  // owned by the lane that holds k = N/2 of its pair
   int k = 0;
   for (long long it = blockIdx.x; it < niter; ++k, it += gridDim.x) {
@@ -562,12 +598,12 @@ k_xpass2(C* __restrict__ work, const C* __restrict__ unyq, const C* __restrict__
 #pragma unroll
         for (int i = 0; i < 16; ++i) {
           const int rr = 2 * i + h;
-          v[i] = cmulc(Wc[pp16(j + 16 * rr)], tw2[rr * 16 + j]);  // inverse twiddle = conj
+          v[i] = cmulc(Wc[pp16(j + 16 * rr)], stage_b_tw(i, j, h));  // inverse twiddle = conj
         }
         dft16<+1>(v);
         if (h) {
 #pragma unroll
-          for (int q = 1; q < 16; ++q) v[q] = cmulc(v[q], tw2[16 * 16 + q]);  // conj W32^q
+          for (int q = 1; q < 16; ++q) v[q] = cmulc(v[q], w32<C>(q));  // conj W32^q
         }
         C* Zc = W + (r * 6 + 3 + c) * SP;
 #pragma unroll
@@ -611,7 +647,8 @@ k_xpass2(C* __restrict__ work, const C* __restrict__ unyq, const C* __restrict__
 #pragma unroll
         for (int q = 0; q < 16; ++q) {
           const int x = pp16(t + M * q);
-          const C za = Za[x], zb = Zb[x];
+          const C za = Za[x];
+          const C zb = ca == cb ? za : Zb[x];  // squares 00, 11, 22: one load
           v[q] = cmk(za.x * zb.x, za.y * zb.y);
         }
         dft16<-1>(v);
@@ -630,12 +667,12 @@ k_xpass2(C* __restrict__ work, const C* __restrict__ unyq, const C* __restrict__
 #pragma unroll
         for (int i = 0; i < 16; ++i) {
           const int rr = 2 * i + h;
-          v[i] = cmul(Wp[pp16(j + 16 * rr)], tw2[rr * 16 + j]);
+          v[i] = cmul(Wp[pp16(j + 16 * rr)], stage_b_tw(i, j, h));
         }
         dft16<-1>(v);
         if (h) {
 #pragma unroll
-          for (int q = 1; q < 16; ++q) v[q] = cmul(v[q], tw2[16 * 16 + q]);
+          for (int q = 1; q < 16; ++q) v[q] = cmul(v[q], w32<C>(q));
         }
 #pragma unroll
         for (int q = 0; q < 16; ++q) {

@@ -51,11 +51,19 @@ def test_two_rank_max_and_rate():
 def test_reference_arm_runs_on_rank0_only(rank):
     env = dict(os.environ, RANK=str(rank), WORLD_SIZE="2", LOCAL_RANK=str(rank))
     r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--n", "16",
-                        "--steps", "1", "--warmup", "1"], capture_output=True, text=True, timeout=600, env=env)
+                        "--steps", "4", "--warmup", "2"], capture_output=True, text=True, timeout=600, env=env)
     assert r.returncode == 0, r.stderr
     if rank == 0:
+        sys.path.insert(0, ROOT)
+        import bench
         line = json.loads(r.stdout.strip().splitlines()[-1])
         assert line["impl"] == "reference" and line["value"] > 0
         assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["cpu_baseline"]["kind"] == "port"
+        # the driver's K and W, the same workload as the GPU arm, and a value consistent with
+        # the timed samples (each one RK3 stage: N^3 / 3 grid-point * steps)
+        assert line["steps"] == 4 and line["warmup"] == 2
+        assert line["config"] == bench.workload_config(16, "fp32", 2)
+        assert line["value"] == pytest.approx(16 ** 3 / 3 / (line["ms_per_step"] / 1e3) / 1e9, rel=1e-9)
+        assert line["fp64_stage"]["value"] > 0
     else:
         assert r.stdout.strip() == ""
