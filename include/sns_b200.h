@@ -13,8 +13,9 @@
  *                   m = i <= N/2 ? i : i - N on each axis (fftw_fft.hpp:45-71).
  * On the device the spectra live on the half spectrum mx in [0, N/2].
  *
- * Supported N: 8, 12, 16, 24, 32, 48, 64, 96, 128, 256, 512 (radix-2/3/4/8 plans);
- * domain [0, 2*pi)^3 so the wavenumber equals the integer mode.
+ * Solver handles (sns_create): N = 8, 12, 16, 24, 32, 48, 64, 96, 128, 256, 512 on the
+ * domain [0, 2*pi)^3, so the wavenumber equals the integer mode.  Any other grid or box
+ * goes through the generic-shape handle (sns_fft3d_*, below).
  */
 #ifndef SNS_B200_H
 #define SNS_B200_H
@@ -270,6 +271,47 @@ const char* sns_server_last_error(const sns_server* s);
  * that is being captured is refused with SNS_ERR_INVALID.  Errors: sns_last_error(NULL). */
 #define SNS_NOALLOC_MAX_N 64
 int sns_forward_r2c_noalloc(int n, const double* dev_physical, double* dev_spectral, void* stream);
+
+/* 1 when the fused passes have a plan for an n^3 grid (sns_create accepts n), else 0. */
+int sns_grid_supported(int n);
+
+/* ---------------------------------------------------------------------------------------
+ * Generic-shape transforms: the FFT-backend contract of FftwFft3D for any grid
+ * (src/fftw_fft.hpp:13-81, src/fftw_fft.cpp:8-85), nx, ny, nz > 1 and box lengths > 0.  The
+ * sns_create handle serves the benchmark domain (cubic, L = 2 pi, N from a fixed list) on the
+ * half spectrum; this handle serves any shape in the reference's own full complex storage.
+ * It holds one complex and one real field (24 bytes per grid point) plus the per-axis
+ * twiddles; the solver calls below add their working set (18 complex and 8 real fields) on
+ * first use.  Axis lengths factor into radices up to 16, run as register butterflies, and
+ * any larger prime, run as a direct DFT of that length (slow for large primes); one CTA's
+ * shared memory bounds an axis to 6400 points.  Errors: sns_fft3d_last_error
+ * (sns_last_error(NULL) for sns_fft3d_create).  Calls are synchronous on the handle's own
+ * stream. */
+typedef struct sns_fft3d sns_fft3d;
+int sns_fft3d_create(int nx, int ny, int nz, double lx, double ly, double lz, sns_fft3d** out);
+int sns_fft3d_destroy(sns_fft3d* h);
+const char* sns_fft3d_last_error(const sns_fft3d* h);
+size_t sns_fft3d_device_bytes(const sns_fft3d* h);
+/* forward: nx*ny*nz real (x fastest) -> 2*nx*ny*nz doubles, unnormalised, sign -1;
+ * backward: 2*nx*ny*nz doubles -> Re(IDFT) / (nx ny nz) (FftwFft3D::forward / backward). */
+int sns_fft3d_forward(sns_fft3d* h, const double* host_physical, double* host_spectral);
+int sns_fft3d_backward(sns_fft3d* h, const double* host_spectral, double* host_physical);
+/* SpectralNavierStokes numerics on this grid, k = 2 pi m / L, in the reference's full layout
+ * (src/spectral_solver.cpp of ovankerm/Spectral_solver):
+ *   rhs: full = 0 -> nonlinear_rhs (:160-240), -i k_j FFT(u_i u_j) with the phase-shift pair
+ *        when dealias = 1 or the plain product when 0, truncated to the ellipsoid mask;
+ *        full = 1 -> rhs (:242-260), minus nu k^2 u_hat, projected, zero mean, truncated;
+ *   step: nsteps Williamson RK3 steps (step_rk3, :262-309) on uhat in place;
+ *   diagnostics: E and max |u| of the physical field, enstrophy 0.5 <|omega|^2>,
+ *        dissipation 2 nu enstrophy, max |k . u_hat| (:311-386);
+ *   product: product_dealiased(a_hat, b_hat) (:122-158), one field each;
+ *   vorticity_slice: |omega| on the physical plane iz, nx*ny doubles (x fastest), the data
+ *        behind write_vorticity_ppm (:421-486). */
+int sns_fft3d_rhs(sns_fft3d* h, double nu, int dealias, int full, const double* const uhat[3], double* const out[3]);
+int sns_fft3d_step(sns_fft3d* h, double nu, int dealias, double dt, int nsteps, double* const uhat[3]);
+int sns_fft3d_diagnostics(sns_fft3d* h, double nu, const double* const uhat[3], double t, sns_diag* out);
+int sns_fft3d_product(sns_fft3d* h, const double* a_hat, const double* b_hat, double* out);
+int sns_fft3d_vorticity_slice(sns_fft3d* h, const double* const uhat[3], int iz, double* host_mag);
 
 /* Test hook: the k-th following call into the handle fails with SNS_ERR_INJECTED
  * (k <= 0 disables).  Exercises the error paths without touching the GPU. */

@@ -5,11 +5,15 @@
 //   physical: N^3 doubles, x fastest, id = ix + n0*(iy + n1*iz)            (fftw_fft.hpp:30-40)
 //   spectral: 2*N^3 doubles, interleaved complex, same order; mode m = i <= n/2 ? i : i - n,
 //             k = 2*pi*m/L                                                  (fftw_fft.hpp:45-71)
-// forward: unnormalised DFT, sign -1; backward: Re(IDFT)/N^3 (fftw_fft.cpp:53-85), for any
+// forward: unnormalised DFT, sign -1; backward: Re(IDFT)/N (fftw_fft.cpp:53-85), for any
 // spectral input, Hermitian or not.  Value semantics, synchronous, one host thread.
 // The transforms run on the GPU that is current when the object is constructed.
 // Errors throw std::runtime_error as the reference's backend does.
-// Grids: cubic, n in {8, 12, 16, 24, 32, 48, 64, 96, 128, 256, 512}.
+// Grids: any nx, ny, nz > 1 (an axis up to 6400 points) and box lengths > 0, like
+// FftwFft3D (fftw_fft.cpp:8-36).  The object holds one complex and one real field on the
+// device (sns_fft3d, 24 bytes per grid point); the fused solver handle of the benchmark
+// domain (cubic, L = 2 pi, n in {8, 12, 16, 24, 32, 48, 64, 96, 128, 256, 512}) is created
+// only when a solver asks for it.
 #pragma once
 
 #include "spectral/mpi_shim.h"
@@ -19,6 +23,7 @@
 #include <vector>
 
 struct sns_handle;
+struct sns_fft3d;
 
 namespace spectral {
 
@@ -82,8 +87,15 @@ class B200Fft3D {
   std::vector<double> forward(const std::vector<double>& physical);
   std::vector<double> backward(const std::vector<double>& spectral);
 
-  // The device handle behind this backend (for solvers that run fused passes on it).
-  sns_handle* handle() const { return handle_; }
+  // The generic-shape transform handle behind this backend (any grid).
+  sns_fft3d* generic() const { return fft_; }
+  // True for the benchmark domain the fused passes serve: cubic, L = 2 pi on every axis,
+  // n with a fused plan.
+  bool fused_domain() const;
+  // The fused solver handle for that domain (created on first use; throws elsewhere).
+  sns_handle* handle();
+  // Device bytes held by the backend (the transform handle, plus the fused handle if made).
+  std::size_t device_bytes() const;
 
  private:
   int mode_of(int idx, int dim) const { return idx <= shape_[dim] / 2 ? idx : idx - shape_[dim]; }
@@ -91,6 +103,7 @@ class B200Fft3D {
   static constexpr double kTwoPi = 6.283185307179586476925286766559005768;
   std::array<int, 3> shape_{};
   std::array<double, 3> lengths_{};
+  sns_fft3d* fft_ = nullptr;
   sns_handle* handle_ = nullptr;
 };
 

@@ -2,12 +2,13 @@
 // (src/spectral_solver.hpp:48-91 of ovankerm/Spectral_solver) with the same constructor,
 // methods, layouts and Diagnostics / SolverProfile records.
 //
-// The time step and the right-hand side run as fused sm_100a passes on the GPU
-// (rhs, nonlinear_rhs, step_rk3, the diagnostics); the pointwise helpers that take and
-// return host vectors (project, truncate, vorticity_hat, kinetic_energy of a physical
-// field) stay on the host as in the reference.  The fused passes need the reference's
-// benchmark domain: cubic grid, L = 2*pi on every axis (wavenumber = integer mode);
-// other domains throw std::runtime_error.
+// The time step, the right-hand side, the diagnostics, product_dealiased and the vorticity
+// slice run on the GPU: as fused sm_100a passes on the reference's benchmark domain (cubic,
+// L = 2*pi on every axis, a planned n, phase-shift dealiasing), and through the
+// generic-shape device path on any other grid, box or product form, as FftwFft3D allows.
+// The pointwise helpers that take and return host vectors (project, truncate,
+// vorticity_hat, kinetic_energy of a physical field, max_spectral_divergence) stay on the
+// host as in the reference.
 #pragma once
 
 #include "spectral/b200_fft.hpp"
@@ -100,7 +101,6 @@ class SpectralNavierStokes {
   bool keep_mode(const SpectralMode& mode) const;
   void zero_mean(VectorSpectral& u_hat) const;
   sns_handle* solver_handle();
-  void require_device_domain() const;
   struct DeviceDiag;
   DeviceDiag device_diagnostics(const VectorSpectral& u_hat);
 
@@ -110,7 +110,8 @@ class SpectralNavierStokes {
   std::vector<std::complex<double>> phase_shift_;
   std::vector<std::uint8_t> keep_mode_mask_;
   SolverProfile profile_;
-  sns_handle* solver_ = nullptr;  // fused-pass handle (created on first use)
+  bool fused_ = false;     // the benchmark domain: fused passes on the backend's solver handle
+  VectorSpectral state_;   // device-resident overloads off that domain: the state on the host
 };
 
 void write_diagnostics_csv(const std::string& path, const std::vector<Diagnostics>& history);

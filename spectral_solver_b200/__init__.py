@@ -4,6 +4,6 @@ The product is native: ``libsns_b200.so`` (sm_100a CUDA kernels behind the C ABI
 ``include/sns_b200.h``) and ``libspectral_b200.so`` (the reference's C++ classes over that
 ABI).  This Python package only binds the C ABI for tests and the benchmark.
 """
-from ._lib import Batch, Server, Solver, SnsError, load  # noqa: F401
+from ._lib import Batch, Fft3D, Server, Solver, SnsError, load  # noqa: F401
 
-__all__ = ["Batch", "Server", "Solver", "SnsError", "load"]
+__all__ = ["Batch", "Fft3D", "Server", "Solver", "SnsError", "load"]

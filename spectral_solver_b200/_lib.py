@@ -98,6 +98,19 @@ SIGNATURES = {
     "sns_server_step": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
                                   C.POINTER(C.c_int), C.POINTER(C.c_size_t)]),
     "sns_server_last_error": (C.c_char_p, [C.c_void_p]),
+    "sns_grid_supported": (C.c_int, [C.c_int]),
+    "sns_fft3d_create": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
+                                   C.POINTER(C.c_void_p)]),
+    "sns_fft3d_destroy": (C.c_int, [C.c_void_p]),
+    "sns_fft3d_last_error": (C.c_char_p, [C.c_void_p]),
+    "sns_fft3d_device_bytes": (C.c_size_t, [C.c_void_p]),
+    "sns_fft3d_forward": (C.c_int, [C.c_void_p, _DP, _DP]),
+    "sns_fft3d_backward": (C.c_int, [C.c_void_p, _DP, _DP]),
+    "sns_fft3d_rhs": (C.c_int, [C.c_void_p, C.c_double, C.c_int, C.c_int, _DPP, _DPP]),
+    "sns_fft3d_step": (C.c_int, [C.c_void_p, C.c_double, C.c_int, C.c_double, C.c_int, _DPP]),
+    "sns_fft3d_diagnostics": (C.c_int, [C.c_void_p, C.c_double, _DPP, C.c_double, C.POINTER(SnsDiag)]),
+    "sns_fft3d_product": (C.c_int, [C.c_void_p, _DP, _DP, _DP]),
+    "sns_fft3d_vorticity_slice": (C.c_int, [C.c_void_p, _DPP, C.c_int, _DP]),
 }
 
 PASS_NAMES = ("p1_zinv_phase", "p2_yinv", "p3_xpass", "p3_nyq", "p4_yfwd", "p5_zfwd", "p5_sweep")
@@ -279,6 +292,96 @@ class Solver:
         self._check(self.lib.sns_autotune(self.h, trial_steps, cache_path.encode() if cache_path else None, out))
         return dict(tma_grid=out[0], xpass_grid=out[1], p5_grid=out[2])
 
+
+
+class Fft3D:
+    """Generic-shape transforms and the legacy solver's numerics (``sns_fft3d_*``): any
+    nx, ny, nz > 1, box lengths lx, ly, lz > 0, the reference's full complex layout (arrays
+    indexed [iz, iy, ix])."""
+
+    def __init__(self, shape, lengths=(2 * np.pi, 2 * np.pi, 2 * np.pi)):
+        self.lib = load()
+        self.shape = tuple(int(v) for v in shape)  # (nx, ny, nz)
+        self.lengths = tuple(float(v) for v in lengths)
+        h = C.c_void_p()
+        rc = self.lib.sns_fft3d_create(*self.shape, *self.lengths, C.byref(h))
+        if rc != SNS_OK:
+            raise SnsError(rc, self.lib.sns_last_error(None).decode())
+        self.h = h
+
+    @property
+    def zyx(self):
+        nx, ny, nz = self.shape
+        return (nz, ny, nx)
+
+    def _check(self, rc):
+        if rc != SNS_OK:
+            raise SnsError(rc, self.lib.sns_fft3d_last_error(self.h).decode())
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.sns_fft3d_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def device_bytes(self) -> int:
+        return int(self.lib.sns_fft3d_device_bytes(self.h))
+
+    def _cplx(self, d):
+        return d.view(np.complex128).reshape(self.zyx)
+
+    def forward(self, phys: np.ndarray) -> np.ndarray:
+        x = np.ascontiguousarray(phys, dtype=np.float64).reshape(-1)
+        out = np.empty(2 * x.size, np.float64)
+        self._check(self.lib.sns_fft3d_forward(self.h, _dptr(x), _dptr(out)))
+        return self._cplx(out)
+
+    def backward(self, spec: np.ndarray) -> np.ndarray:
+        x = full_to_interleaved(spec)
+        out = np.empty(x.size // 2, np.float64)
+        self._check(self.lib.sns_fft3d_backward(self.h, _dptr(x), _dptr(out)))
+        return out.reshape(self.zyx)
+
+    def rhs(self, u_full, nu: float, dealias: bool = True, full: bool = True):
+        ins = [full_to_interleaved(c) for c in u_full]
+        outs = [np.empty_like(a) for a in ins]
+        self._check(self.lib.sns_fft3d_rhs(self.h, nu, int(dealias), int(full), _arr3(ins), _arr3(outs)))
+        return [self._cplx(a) for a in outs]
+
+    def step(self, u_full, nu: float, dt: float, nsteps: int = 1, dealias: bool = True):
+        arrs = [full_to_interleaved(c).copy() for c in u_full]
+        self._check(self.lib.sns_fft3d_step(self.h, nu, int(dealias), dt, nsteps, _arr3(arrs)))
+        return [self._cplx(a) for a in arrs]
+
+    def diagnostics(self, u_full, nu: float, t: float = 0.0) -> dict:
+        ins = [full_to_interleaved(c) for c in u_full]
+        d = SnsDiag()
+        self._check(self.lib.sns_fft3d_diagnostics(self.h, nu, _arr3(ins), t, C.byref(d)))
+        return d.as_dict()
+
+    def product(self, a_hat, b_hat):
+        a, b = full_to_interleaved(a_hat), full_to_interleaved(b_hat)
+        out = np.empty_like(a)
+        self._check(self.lib.sns_fft3d_product(self.h, _dptr(a), _dptr(b), _dptr(out)))
+        return self._cplx(out)
+
+    def vorticity_slice(self, u_full, iz: int) -> np.ndarray:
+        ins = [full_to_interleaved(c) for c in u_full]
+        nx, ny, _ = self.shape
+        out = np.empty(nx * ny, np.float64)
+        self._check(self.lib.sns_fft3d_vorticity_slice(self.h, _arr3(ins), iz, _dptr(out)))
+        return out.reshape(ny, nx)
 
 
 class _BorrowedSolver(Solver):

@@ -582,6 +582,8 @@ extern "C" {
 
 const char* sns_version(void) { return "sns_b200 0.2 (sm_100a, fp64 plain form, fp32 precision form)"; }
 
+int sns_grid_supported(int n) { return n > 0 && sns::ops_for(n, 0) != nullptr ? 1 : 0; }
+
 size_t sns_bytes_required(int n, int precision) {
   if (n <= 0 || (precision != SNS_PRECISION_FP64 && precision != SNS_PRECISION_FP32)) return 0;
   return 18 * field_bytes(n, precision) + comp_bytes(n, precision) + partial_slots(n) * sizeof(double) +

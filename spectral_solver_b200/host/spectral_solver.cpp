@@ -1,7 +1,12 @@
 // SpectralNavierStokes over B200Fft3D (the reference's src/spectral_solver.cpp:35-488 API).
 //
-// rhs / nonlinear_rhs / step_rk3 / the spectral diagnostics go through the fused device
-// passes of the backend's handle; host-vector helpers keep the reference's semantics.
+// rhs / nonlinear_rhs / step_rk3 / the diagnostics / product_dealiased / the vorticity slice
+// run on the GPU: on the benchmark domain (cubic, L = 2 pi, a planned n, phase-shift
+// dealiasing) through the fused passes of the backend's solver handle, on every other domain
+// (any shape, any lengths, either product form) through the generic-shape device path
+// (sns_fft3d_*).  The remaining host-vector helpers (project, truncate, vorticity_hat,
+// kinetic_energy of a physical field, max_spectral_divergence) keep the reference's
+// semantics on the host.
 #include "spectral/spectral_solver.hpp"
 
 #include "sns_b200.h"
@@ -31,6 +36,9 @@ void put(std::vector<double>& a, std::size_t id, std::complex<double> z) {
 void check(int rc, sns_handle* h, const char* what) {
   if (rc != SNS_OK) throw std::runtime_error(std::string(what) + ": " + sns_last_error(h));
 }
+void check(int rc, sns_fft3d* h, const char* what) {
+  if (rc != SNS_OK) throw std::runtime_error(std::string(what) + ": " + sns_fft3d_last_error(h));
+}
 
 VectorSpectral zeros_spectral(std::size_t n) { return {ScalarSpectral(n, 0.0), ScalarSpectral(n, 0.0), ScalarSpectral(n, 0.0)}; }
 
@@ -55,22 +63,12 @@ SpectralNavierStokes::SpectralNavierStokes(std::array<int, 3> shape, std::array<
     phase_shift_[id / 2] = std::exp(std::complex<double>(0.0, m.kx * hx + m.ky * hy + m.kz * hz));
     keep_mode_mask_[id / 2] = keep_mode(m) ? 1 : 0;
   });
+  fused_ = phase_shift_dealiasing_ && fft_.fused_domain();
 }
 
 SpectralNavierStokes::~SpectralNavierStokes() = default;
 
-void SpectralNavierStokes::require_device_domain() const {
-  const auto& L = fft_.lengths();
-  for (double l : L) {
-    if (std::abs(l - 2.0 * kPi) > 1e-12 * 2.0 * kPi)
-      throw std::runtime_error("the fused B200 passes need the [0, 2*pi)^3 domain (wavenumber = integer mode)");
-  }
-  if (!phase_shift_dealiasing_)
-    throw std::runtime_error("the fused B200 passes implement the phase-shift dealiased product");
-}
-
 sns_handle* SpectralNavierStokes::solver_handle() {
-  require_device_domain();
   sns_handle* h = fft_.handle();
   check(sns_set_viscosity(h, nu_), h, "SpectralNavierStokes");
   return h;
@@ -123,38 +121,28 @@ void SpectralNavierStokes::truncate(VectorSpectral& u_hat) const {
 }
 
 ScalarSpectral SpectralNavierStokes::product_dealiased(const ScalarSpectral& a_hat, const ScalarSpectral& b_hat) {
-  // device transforms; the two products and the combine are pointwise host work, as in
-  // src/spectral_solver.cpp:122-158
-  const auto a = fft_.backward(a_hat);
-  const auto b = fft_.backward(b_hat);
-  ScalarPhysical p(a.size());
-  for (std::size_t i = 0; i < p.size(); ++i) p[i] = a[i] * b[i];
-  const auto c0 = fft_.forward(p);
-  ScalarSpectral as = a_hat, bs = b_hat;
-  for (std::size_t m = 0; m < phase_shift_.size(); ++m) {
-    put(as, 2 * m, at(as, 2 * m) * phase_shift_[m]);
-    put(bs, 2 * m, at(bs, 2 * m) * phase_shift_[m]);
-  }
-  const auto sa = fft_.backward(as);
-  const auto sb = fft_.backward(bs);
-  for (std::size_t i = 0; i < p.size(); ++i) p[i] = sa[i] * sb[i];
-  const auto cs = fft_.forward(p);
-  ScalarSpectral out(c0.size(), 0.0);
-  for (std::size_t m = 0; m < phase_shift_.size(); ++m) {
-    if (!keep_mode_mask_[m]) continue;
-    put(out, 2 * m, 0.5 * (at(c0, 2 * m) + at(cs, 2 * m) * std::conj(phase_shift_[m])));
-  }
+  // both products, their transforms and the combine on the device (src/spectral_solver.cpp:122-158)
+  if (a_hat.size() != fft_.spectral_storage_size() || b_hat.size() != fft_.spectral_storage_size())
+    throw std::runtime_error("spectral field has wrong storage size");
+  ScalarSpectral out(fft_.spectral_storage_size(), 0.0);
+  sns_fft3d* g = fft_.generic();
+  check(sns_fft3d_product(g, a_hat.data(), b_hat.data(), out.data()), g, "SpectralNavierStokes::product_dealiased");
   return out;
 }
 
 VectorSpectral SpectralNavierStokes::nonlinear_rhs(const VectorSpectral& u_hat) {
   const auto t0 = Clock::now();
   profile_.nonlinear_calls += 1;
-  sns_handle* h = solver_handle();
   VectorSpectral out = zeros_spectral(fft_.spectral_storage_size());
   const double* in[3] = {u_hat[0].data(), u_hat[1].data(), u_hat[2].data()};
   double* o[3] = {out[0].data(), out[1].data(), out[2].data()};
-  check(sns_nonlinear(h, in, o), h, "SpectralNavierStokes::nonlinear_rhs");
+  if (fused_) {
+    sns_handle* h = solver_handle();
+    check(sns_nonlinear(h, in, o), h, "SpectralNavierStokes::nonlinear_rhs");
+  } else {
+    sns_fft3d* g = fft_.generic();
+    check(sns_fft3d_rhs(g, nu_, phase_shift_dealiasing_ ? 1 : 0, 0, in, o), g, "SpectralNavierStokes::nonlinear_rhs");
+  }
   profile_.nonlinear_rhs += seconds_since(t0);
   return out;
 }
@@ -162,11 +150,16 @@ VectorSpectral SpectralNavierStokes::nonlinear_rhs(const VectorSpectral& u_hat) 
 VectorSpectral SpectralNavierStokes::rhs(const VectorSpectral& u_hat) {
   const auto t0 = Clock::now();
   profile_.rhs_calls += 1;
-  sns_handle* h = solver_handle();
   VectorSpectral out = zeros_spectral(fft_.spectral_storage_size());
   const double* in[3] = {u_hat[0].data(), u_hat[1].data(), u_hat[2].data()};
   double* o[3] = {out[0].data(), out[1].data(), out[2].data()};
-  check(sns_rhs(h, in, o), h, "SpectralNavierStokes::rhs");
+  if (fused_) {
+    sns_handle* h = solver_handle();
+    check(sns_rhs(h, in, o), h, "SpectralNavierStokes::rhs");
+  } else {
+    sns_fft3d* g = fft_.generic();
+    check(sns_fft3d_rhs(g, nu_, phase_shift_dealiasing_ ? 1 : 0, 1, in, o), g, "SpectralNavierStokes::rhs");
+  }
   profile_.rhs += seconds_since(t0);
   return out;
 }
@@ -175,13 +168,21 @@ VectorSpectral SpectralNavierStokes::step_rk3(const VectorSpectral& u_hat, doubl
   (void)t;
   const auto t0 = Clock::now();
   profile_.steps += 1;
-  sns_handle* h = solver_handle();
-  const double* in[3] = {u_hat[0].data(), u_hat[1].data(), u_hat[2].data()};
-  check(sns_set_state(h, in), h, "SpectralNavierStokes::step_rk3");
-  check(sns_step(h, dt, 1), h, "SpectralNavierStokes::step_rk3");
-  VectorSpectral out = zeros_spectral(fft_.spectral_storage_size());
-  double* o[3] = {out[0].data(), out[1].data(), out[2].data()};
-  check(sns_get_state(h, o), h, "SpectralNavierStokes::step_rk3");
+  VectorSpectral out;
+  if (fused_) {
+    sns_handle* h = solver_handle();
+    const double* in[3] = {u_hat[0].data(), u_hat[1].data(), u_hat[2].data()};
+    check(sns_set_state(h, in), h, "SpectralNavierStokes::step_rk3");
+    check(sns_step(h, dt, 1), h, "SpectralNavierStokes::step_rk3");
+    out = zeros_spectral(fft_.spectral_storage_size());
+    double* o[3] = {out[0].data(), out[1].data(), out[2].data()};
+    check(sns_get_state(h, o), h, "SpectralNavierStokes::step_rk3");
+  } else {
+    out = u_hat;
+    double* o[3] = {out[0].data(), out[1].data(), out[2].data()};
+    sns_fft3d* g = fft_.generic();
+    check(sns_fft3d_step(g, nu_, phase_shift_dealiasing_ ? 1 : 0, dt, 1, o), g, "SpectralNavierStokes::step_rk3");
+  }
   profile_.step_rk3 += seconds_since(t0);
   return out;
 }
@@ -195,11 +196,16 @@ double SpectralNavierStokes::kinetic_energy(const VectorPhysical& u) const {
 }
 
 SpectralNavierStokes::DeviceDiag SpectralNavierStokes::device_diagnostics(const VectorSpectral& u_hat) {
-  sns_handle* h = solver_handle();
   const double* in[3] = {u_hat[0].data(), u_hat[1].data(), u_hat[2].data()};
-  check(sns_set_state(h, in), h, "SpectralNavierStokes diagnostics");
   DeviceDiag d{};
-  check(sns_diagnostics(h, 0.0, &d.d), h, "SpectralNavierStokes diagnostics");
+  if (fused_) {
+    sns_handle* h = solver_handle();
+    check(sns_set_state(h, in), h, "SpectralNavierStokes diagnostics");
+    check(sns_diagnostics(h, 0.0, &d.d), h, "SpectralNavierStokes diagnostics");
+  } else {
+    sns_fft3d* g = fft_.generic();
+    check(sns_fft3d_diagnostics(g, nu_, in, 0.0, &d.d), g, "SpectralNavierStokes diagnostics");
+  }
   return d;
 }
 
@@ -245,30 +251,55 @@ Diagnostics SpectralNavierStokes::diagnostics(const VectorSpectral& u_hat, doubl
   return row;
 }
 
+// On the benchmark domain the state stays in HBM between calls; elsewhere it is kept on the
+// host and each step_rk3(dt, n) uploads it once, takes the n steps on the device and reads
+// it back.
 void SpectralNavierStokes::load_state(const VectorSpectral& u_hat) {
-  sns_handle* h = solver_handle();
-  const double* in[3] = {u_hat[0].data(), u_hat[1].data(), u_hat[2].data()};
-  check(sns_set_state(h, in), h, "SpectralNavierStokes::load_state");
+  if (fused_) {
+    sns_handle* h = solver_handle();
+    const double* in[3] = {u_hat[0].data(), u_hat[1].data(), u_hat[2].data()};
+    check(sns_set_state(h, in), h, "SpectralNavierStokes::load_state");
+  } else {
+    for (const auto& c : u_hat)
+      if (c.size() != fft_.spectral_storage_size()) throw std::runtime_error("spectral field has wrong storage size");
+    state_ = u_hat;
+  }
 }
 
 void SpectralNavierStokes::step_rk3(double dt, int nsteps) {
   const auto t0 = Clock::now();
-  sns_handle* h = solver_handle();
-  check(sns_step(h, dt, nsteps), h, "SpectralNavierStokes::step_rk3");
+  if (fused_) {
+    sns_handle* h = solver_handle();
+    check(sns_step(h, dt, nsteps), h, "SpectralNavierStokes::step_rk3");
+  } else {
+    if (state_[0].empty()) throw std::runtime_error("SpectralNavierStokes::step_rk3: no state loaded");
+    double* o[3] = {state_[0].data(), state_[1].data(), state_[2].data()};
+    sns_fft3d* g = fft_.generic();
+    check(sns_fft3d_step(g, nu_, phase_shift_dealiasing_ ? 1 : 0, dt, nsteps, o), g,
+          "SpectralNavierStokes::step_rk3");
+  }
   profile_.steps += nsteps;
   profile_.step_rk3 += seconds_since(t0);
 }
 
 Diagnostics SpectralNavierStokes::diagnostics(double t) {
   const auto t0 = Clock::now();
-  sns_handle* h = solver_handle();
   sns_diag d{};
-  check(sns_diagnostics(h, t, &d), h, "SpectralNavierStokes::diagnostics");
+  if (fused_) {
+    sns_handle* h = solver_handle();
+    check(sns_diagnostics(h, t, &d), h, "SpectralNavierStokes::diagnostics");
+  } else {
+    if (state_[0].empty()) throw std::runtime_error("SpectralNavierStokes::diagnostics: no state loaded");
+    const double* in[3] = {state_[0].data(), state_[1].data(), state_[2].data()};
+    sns_fft3d* g = fft_.generic();
+    check(sns_fft3d_diagnostics(g, nu_, in, t, &d), g, "SpectralNavierStokes::diagnostics");
+  }
   profile_.diagnostics += seconds_since(t0);
   return Diagnostics{t, d.kinetic_energy, 2.0 * nu_ * d.enstrophy, d.enstrophy, d.max_spectral_divergence};
 }
 
 VectorSpectral SpectralNavierStokes::state() {
+  if (!fused_) return state_;
   sns_handle* h = solver_handle();
   VectorSpectral out = zeros_spectral(fft_.spectral_storage_size());
   double* o[3] = {out[0].data(), out[1].data(), out[2].data()};
@@ -296,19 +327,19 @@ void write_diagnostics_csv(const std::string& path, const std::vector<Diagnostic
 }
 
 void write_vorticity_ppm(const std::string& path, SpectralNavierStokes& solver, const VectorSpectral& u_hat) {
-  // |omega| on the mid z plane as a binary PPM (src/spectral_solver.cpp:421-486)
-  const auto w = solver.to_physical(solver.vorticity_hat(u_hat));
+  // |omega| on the mid z plane as a binary PPM (src/spectral_solver.cpp:421-486): omega_hat,
+  // its inverse transforms and the slice's magnitudes on the device; only the n0 x n1 slice
+  // comes back, and the palette below is the reference's
   const auto& n = solver.fft().shape();
   const int iz = n[2] / 2;
   std::vector<double> mag(static_cast<std::size_t>(n[0]) * n[1]);
+  for (const auto& c : u_hat)
+    if (c.size() != solver.fft().spectral_storage_size()) throw std::runtime_error("spectral field has wrong storage size");
+  const double* in[3] = {u_hat[0].data(), u_hat[1].data(), u_hat[2].data()};
+  sns_fft3d* g = solver.fft().generic();
+  check(sns_fft3d_vorticity_slice(g, in, iz, mag.data()), g, "write_vorticity_ppm");
   double vmax = 0.0;
-  for (int iy = 0; iy < n[1]; ++iy)
-    for (int ix = 0; ix < n[0]; ++ix) {
-      const std::size_t src = static_cast<std::size_t>(ix + n[0] * (iy + n[1] * iz));
-      const double v = std::sqrt(w[0][src] * w[0][src] + w[1][src] * w[1][src] + w[2][src] * w[2][src]);
-      mag[static_cast<std::size_t>(ix + n[0] * iy)] = v;
-      vmax = std::max(vmax, v);
-    }
+  for (double v : mag) vmax = std::max(vmax, v);
   if (vmax == 0.0) vmax = 1.0;
   std::ofstream f(path, std::ios::binary);
   f << "P6\n" << n[0] << " " << n[1] << "\n255\n";

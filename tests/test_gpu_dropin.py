@@ -36,8 +36,10 @@ def run_cli(args, outdir, timeout=900):
     return rows, r.stdout
 
 
-def test_reference_cpp_tests_on_b200_backend():
-    r = subprocess.run([os.path.join(BIN, "spectral_ns_b200")], capture_output=True, text=True, timeout=300)
+def test_reference_cpp_tests_on_b200_backend(tmp_path):
+    # the binary writes its vorticity PPMs into the working directory
+    r = subprocess.run([os.path.join(BIN, "spectral_ns_b200")], capture_output=True, text=True, timeout=300,
+                       cwd=tmp_path)
     assert r.returncode == 0, r.stderr
     assert "all C++ spectral tests passed" in r.stdout
 
