@@ -217,13 +217,17 @@ int sns_autotune(sns_handle* h, int trial_steps, const char* cache_path, int* ou
 
 /* ---------------------------------------------------------------------------------------
  * Serving with continuous batching (no counterpart in the reference).  Requests queue on
- * the host; each sns_server_step (one tick) admits queued requests in arrival order while
- * their device bytes fit the HBM budget, advances every resident solve on its own stream
- * (so their work overlaps on the device) -- the largest resident solve by one step, smaller
- * ones by N_max^3/N^3 steps (at most 64) -- and retires the solves that reached their
- * horizon (final diagnostics returned, memory freed), so requests that arrive while others
- * run are admitted as memory frees up.  Each solve's step is fixed at admission by the CFL
- * rule on its initial field; each result is bitwise that of the same request solved alone. */
+ * the host; each sns_server_step (one tick, which never waits for GPU work) admits queued
+ * requests in arrival order while their device bytes fit the HBM budget, queues the next
+ * batch of steps of every resident solve that has fewer than two batches in flight, on the
+ * solve's own stream (so their work overlaps on the device) -- the largest resident solve by
+ * one step, smaller ones by N_max^3/N^3 steps (at most 64) -- and retires the solves whose
+ * last step has completed (final diagnostics returned).  A retired solve's device memory
+ * is kept in an idle pool and the next request of the same N re-initialises it in place, so
+ * a steady stream admits and retires without cudaMalloc / cudaFree; the budget counts
+ * resident and idle memory, and idle handles of another N are freed only to make room.
+ * Each solve's step is fixed at admission by the CFL rule on its initial field; each result
+ * is bitwise that of the same request solved alone. */
 typedef struct sns_server sns_server;
 
 typedef struct sns_request {
@@ -254,6 +258,10 @@ int sns_server_submit(sns_server* s, const sns_request* r, int64_t* out_id);
 int sns_server_step(sns_server* s, sns_result* done, int max_done, int* ndone, int* resident, int* queued,
                     size_t* bytes_in_use);
 const char* sns_server_last_error(const sns_server* s);
+/* Pool figures: idle_bytes (may be NULL) the device bytes of retired handles kept for reuse;
+ * handles_created (may be NULL) how many handles the server has allocated so far (a request
+ * that found an idle handle of its N allocated nothing). */
+int sns_server_stats(const sns_server* s, size_t* idle_bytes, long long* handles_created);
 
 /* Forward transform that allocates no device memory (no counterpart in the reference).
  * For callers that cannot let a library call cudaMalloc: applications that reserve the

@@ -99,6 +99,7 @@ SIGNATURES = {
                                   C.POINTER(C.c_int), C.POINTER(C.c_size_t)]),
     "sns_server_last_error": (C.c_char_p, [C.c_void_p]),
     "sns_grid_supported": (C.c_int, [C.c_int]),
+    "sns_server_stats": (C.c_int, [C.c_void_p, C.POINTER(C.c_size_t), C.POINTER(C.c_longlong)]),
     "sns_fft3d_create": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
                                    C.POINTER(C.c_void_p)]),
     "sns_fft3d_destroy": (C.c_int, [C.c_void_p]),
@@ -488,6 +489,12 @@ class Server:
         out = [dict(id=done[i].id, n=done[i].n, steps=done[i].steps, dt=done[i].dt, final=done[i].final.as_dict())
                for i in range(nd.value)]
         return out, res.value, q.value, used.value
+
+    def stats(self) -> dict:
+        """Idle-pool bytes and the number of handles the server has allocated."""
+        idle, made = C.c_size_t(), C.c_longlong()
+        self._check(self.lib.sns_server_stats(self.s, C.byref(idle), C.byref(made)))
+        return {"idle_bytes": idle.value, "handles_created": made.value}
 
     def close(self):
         if getattr(self, "s", None):

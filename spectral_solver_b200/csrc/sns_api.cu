@@ -497,6 +497,38 @@ void velocity_reductions(sns_handle* h) {
   sns::launch_reduce(h->partials + 1, rows, 2, 1, h->red + 1, h->stream);
 }
 
+// The initial state on the handle's own memory: Taylor-Green at cell centres -> forward
+// transform -> + seeded perturbation -> project_truncate; g, the work fields and the FP32
+// form's compensation words zeroed.  Allocates nothing (sns_create and the server's reuse of
+// a retired handle both run it).
+void initial_field(sns_handle* h, uint64_t seed, double pert_amp, int pert_kmax) {
+  const sns::Ops* ops = h->ops;
+  const size_t fb = h->fbytes;
+  ck(cudaMemsetAsync(h->state, 0, 6 * fb, h->stream), "memset");
+  ck(cudaMemsetAsync(h->work, 0, 12 * fb, h->stream), "memset");
+  if (h->ulo) ck(cudaMemsetAsync(h->ulo, 0, comp_bytes(h->n, h->precision), h->stream), "memset");
+  double* phys = reinterpret_cast<double*>(h->wf(6));
+  sns::launch_tgv_init(phys, h->g, h->stream);
+  ops->xpass_r2c(phys, h->u(), 2, h->tw, h->g, h->stream);  // w = 0: its spectrum stays zero
+  ops->ypass(h->u(), 2, -1, h->tiles_all(), h->tw, h->g, h->stream);
+  ops->zpass(h->u(), h->u(), 2, -1, h->tiles_all(), 1.0, h->tw, h->g, h->stream);
+  std::vector<long long> idx;
+  std::vector<double2> val;
+  perturbation_entries(h->n, seed, pert_amp, pert_kmax, h->g, idx, val);
+  if (!idx.empty()) {
+    long long* d_idx = reinterpret_cast<long long*>(h->wf(8));
+    double2* d_val = reinterpret_cast<double2*>(h->wf(9));
+    ck(cudaMemcpyAsync(d_idx, idx.data(), idx.size() * sizeof(long long), cudaMemcpyHostToDevice, h->stream), "p");
+    ck(cudaMemcpyAsync(d_val, val.data(), val.size() * sizeof(double2), cudaMemcpyHostToDevice, h->stream), "p");
+    sns::launch_add_sparse(h->u(), h->precision, d_idx, d_val, (int)idx.size(), h->stream);
+    ck(cudaStreamSynchronize(h->stream), "perturbation");
+  }
+  sns::launch_project_truncate(h->u(), h->precision, h->g, h->stream);
+  ck(cudaMemsetAsync(h->work, 0, 12 * fb, h->stream), "memset");
+  h->nyq_clean = true;
+  h->sphere_clean = true;  // project_truncate zeroed every mode outside the sphere
+}
+
 template <class F>
 int guarded(sns_handle* h, F&& f) {
   if (h == nullptr) return SNS_ERR_INVALID;
@@ -575,6 +607,21 @@ bool set_launch_shape(sns_handle* h, const int* cfg) {
   return true;
 }
 void set_handle_error(sns_handle* h, const char* msg) { h->err = msg; }
+// A handle returned to its creation state for a new solve of the same N and precision
+// (viscosity, seed and perturbation of the new solve), on its own memory: no allocation.
+int reset_handle(sns_handle* h, double nu, uint64_t seed, double pert_amp, int pert_kmax) {
+  return guarded(h, [&] {
+    if (!(nu >= 0.0) || !std::isfinite(nu)) throw SnsError(SNS_ERR_INVALID, "viscosity must be finite and >= 0");
+    if (!(pert_amp >= 0.0) || (pert_amp > 0.0 && 2 * pert_kmax >= h->n))
+      throw SnsError(SNS_ERR_INVALID, "perturbation amplitude must be >= 0 and kmax below N/2");
+    h->nu = nu;
+    h->form = 0;
+    h->prune = true;
+    h->comp = h->ulo != nullptr;
+    initial_field(h, seed, pert_amp, pert_kmax);
+    sync(h, "reset");
+  });
+}
 
 }  // namespace sns
 
@@ -718,26 +765,7 @@ int sns_create(int n, double nu, int precision, int viscous_mode, uint64_t seed,
     const auto ph = phase_table(n);
     upload_table(h->tw, tw, precision, h->stream);
     upload_table(h->phase, ph, precision, h->stream);
-    // Initial field: TGV at cell centres -> forward transform -> + perturbation -> project_truncate.
-    double* phys = reinterpret_cast<double*>(h->wf(6));
-    sns::launch_tgv_init(phys, h->g, h->stream);
-    ops->xpass_r2c(phys, h->u(), 2, h->tw, h->g, h->stream);  // w = 0: its spectrum stays zero
-    ops->ypass(h->u(), 2, -1, h->tiles_all(), h->tw, h->g, h->stream);
-    ops->zpass(h->u(), h->u(), 2, -1, h->tiles_all(), 1.0, h->tw, h->g, h->stream);
-    std::vector<long long> idx;
-    std::vector<double2> val;
-    perturbation_entries(n, seed, pert_amp, pert_kmax, h->g, idx, val);
-    if (!idx.empty()) {
-      long long* d_idx = reinterpret_cast<long long*>(h->wf(8));
-      double2* d_val = reinterpret_cast<double2*>(h->wf(9));
-      ck(cudaMemcpyAsync(d_idx, idx.data(), idx.size() * sizeof(long long), cudaMemcpyHostToDevice, h->stream), "p");
-      ck(cudaMemcpyAsync(d_val, val.data(), val.size() * sizeof(double2), cudaMemcpyHostToDevice, h->stream), "p");
-      sns::launch_add_sparse(h->u(), precision, d_idx, d_val, (int)idx.size(), h->stream);
-      ck(cudaStreamSynchronize(h->stream), "perturbation");
-    }
-    sns::launch_project_truncate(h->u(), precision, h->g, h->stream);
-    h->sphere_clean = true;  // project_truncate zeroed every mode outside the sphere
-    ck(cudaMemsetAsync(h->work, 0, 12 * fb, h->stream), "memset");
+    initial_field(h, seed, pert_amp, pert_kmax);
     sync(h, "sns_create");
   } catch (const SnsError& e) {
     g_create_error = e.msg;

@@ -141,6 +141,8 @@ int finish_handle(sns_handle* h, const char* what);  // sync + device error word
 const char* handle_error(const sns_handle* h);
 bool set_launch_shape(sns_handle* h, const int* cfg);  // {tma_grid, x2_grid, p5_grid}
 void set_handle_error(sns_handle* h, const char* msg);
+// the handle back in its creation state for a new solve (same N and precision), no allocation
+int reset_handle(sns_handle* h, double nu, uint64_t seed, double pert_amp, int pert_kmax);
 
 // Host helpers shared by the C-ABI files (sns_api.cu).
 void fill_twiddles(int L, double2* tw);        // exp(-2*pi*i*t/L), t < L

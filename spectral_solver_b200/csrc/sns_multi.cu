@@ -8,6 +8,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <array>
 #include <cmath>
 #include <cstdint>
@@ -152,26 +153,45 @@ int batch_finish(sns_batch* b, const char* what) {
 
 // ---------------------------------------------------------------------------------------
 // Continuous-batching server.
+//
+// Memory: a solve's handle (fields, tables, stream) is not freed when the solve retires; it
+// joins an idle pool keyed by N and the next request of that N takes it over (its state
+// re-initialised in place), so a steady stream admits and retires without cudaMalloc or
+// cudaFree, which would synchronise the whole device.  The budget counts resident and idle
+// handles; an idle handle of another N is freed only when a request needs its room.
+// Time: a tick never waits for GPU work.  It launches a resident solve's next batch of
+// steps only when at most one earlier batch is still in flight (two batches queued per
+// solve keep the device busy between ticks), and retires a solve once the event after its
+// last step has completed, so requests are admitted and initialised while the others run.
 struct sns_server {
   struct Pending {
     int64_t id;
     sns_request req;
   };
-  struct Resident {
+  struct Slot {  // a handle with its own completion events, resident or idle
     sns_handle* h = nullptr;
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    size_t bytes = 0;
+    int n = 0;
+  };
+  struct Resident {
+    Slot slot;
     cudaGraphExec_t step = nullptr;  // one full step of size dt
     int64_t id = 0;
     sns_request req{};
     double dt = 0.0, t = 0.0;
     int steps = 0;
-    size_t bytes = 0;
+    int head = 0;     // next event slot to record
+    int pending = 0;  // recorded batches not yet seen complete (0..2)
   };
-  size_t budget = 0, used = 0;
+  size_t budget = 0, used = 0, idle_bytes = 0;
   int precision = 0;
   int device = 0;
   int64_t next_id = 1;
+  long long allocations = 0;  // handles created (the pool's misses)
   std::deque<Pending> queue;
   std::vector<Resident> resident;
+  std::vector<Slot> idle;
   std::deque<sns_result> done;  // finished, not yet returned
   std::string err;
 };
@@ -183,12 +203,36 @@ int server_fail(sns_server* s, int code, const std::string& msg) {
   return code;
 }
 
+void free_slot(sns_server::Slot& sl) {
+  for (cudaEvent_t& e : sl.ev)
+    if (e) cudaEventDestroy(e);
+  if (sl.h) sns_destroy(sl.h);
+  sl = sns_server::Slot{};
+}
+
+// A retired solve's handle goes to the idle pool (no device memory is released).
 void retire(sns_server* s, size_t i) {
   sns_server::Resident& r = s->resident[i];
   if (r.step) cudaGraphExecDestroy(r.step);
-  if (r.h) sns_destroy(r.h);
-  s->used -= r.bytes;
+  s->used -= r.slot.bytes;
+  s->idle_bytes += r.slot.bytes;
+  s->idle.push_back(r.slot);
   s->resident.erase(s->resident.begin() + (long)i);
+}
+
+// Room for `bytes` more under the budget, freeing idle handles of other sizes (largest
+// first) if that makes it fit; false if it does not fit even then.
+bool make_room(sns_server* s, size_t bytes) {
+  if (s->used + s->idle_bytes + bytes <= s->budget) return true;
+  if (s->used + bytes > s->budget) return false;
+  std::sort(s->idle.begin(), s->idle.end(),
+            [](const sns_server::Slot& a, const sns_server::Slot& b) { return a.bytes < b.bytes; });
+  while (!s->idle.empty() && s->used + s->idle_bytes + bytes > s->budget) {
+    s->idle_bytes -= s->idle.back().bytes;
+    free_slot(s->idle.back());
+    s->idle.pop_back();
+  }
+  return s->used + s->idle_bytes + bytes <= s->budget;
 }
 
 // Admit queued requests in arrival order while their device bytes fit the budget.
@@ -200,34 +244,70 @@ int admit(sns_server* s) {
       s->queue.pop_front();
       return server_fail(s, SNS_ERR_UNSUPPORTED, "request " + std::to_string(p.id) + ": unsupported grid size");
     }
-    if (s->used + bytes > s->budget) {
-      if (s->resident.empty())
-        return server_fail(s, SNS_ERR_NOMEM, "request " + std::to_string(p.id) + " needs " + std::to_string(bytes) +
-                                                 " bytes, more than the whole HBM budget");
-      return SNS_OK;  // waits until memory frees up
-    }
+    if (bytes > s->budget)
+      return server_fail(s, SNS_ERR_NOMEM, "request " + std::to_string(p.id) + " needs " + std::to_string(bytes) +
+                                               " bytes, more than the whole HBM budget");
     sns_server::Resident r;
     r.id = p.id;
     r.req = p.req;
-    r.bytes = bytes;
-    int rc = sns_create(p.req.n, p.req.nu, s->precision, SNS_VISCOUS_EXPLICIT, p.req.seed, p.req.pert_amp,
-                        p.req.pert_kmax, &r.h);
-    if (rc == SNS_ERR_NOMEM && !s->resident.empty()) return SNS_OK;  // the device itself is full: wait
-    if (rc != SNS_OK) {
-      s->queue.pop_front();
-      return server_fail(s, rc, "request " + std::to_string(p.id) + ": " + sns_last_error(nullptr));
+    // an idle handle of this N: reuse it in place
+    size_t k = 0;
+    while (k < s->idle.size() && s->idle[k].n != p.req.n) ++k;
+    int rc = SNS_OK;
+    if (k < s->idle.size()) {
+      r.slot = s->idle[k];
+      s->idle.erase(s->idle.begin() + (long)k);
+      s->idle_bytes -= r.slot.bytes;
+      rc = sns::reset_handle(r.slot.h, p.req.nu, p.req.seed, p.req.pert_amp, p.req.pert_kmax);
+      if (rc != SNS_OK) {
+        const std::string msg = sns_last_error(r.slot.h);
+        free_slot(r.slot);
+        s->queue.pop_front();
+        return server_fail(s, rc, "request " + std::to_string(p.id) + ": " + msg);
+      }
+    } else {
+      if (!make_room(s, bytes)) return SNS_OK;  // waits until retirements free memory
+      rc = sns_create(p.req.n, p.req.nu, s->precision, SNS_VISCOUS_EXPLICIT, p.req.seed, p.req.pert_amp,
+                      p.req.pert_kmax, &r.slot.h);
+      if (rc == SNS_ERR_NOMEM && !s->resident.empty()) return SNS_OK;  // the device itself is full: wait
+      if (rc != SNS_OK) {
+        s->queue.pop_front();
+        return server_fail(s, rc, "request " + std::to_string(p.id) + ": " + sns_last_error(nullptr));
+      }
+      ++s->allocations;
+      r.slot.bytes = bytes;
+      r.slot.n = p.req.n;
+      cudaError_t e = cudaEventCreateWithFlags(&r.slot.ev[0], cudaEventDisableTiming);
+      if (e == cudaSuccess) e = cudaEventCreateWithFlags(&r.slot.ev[1], cudaEventDisableTiming);
+      if (e != cudaSuccess) {
+        free_slot(r.slot);
+        s->queue.pop_front();
+        return server_fail(s, SNS_ERR_CUDA, cuda_msg("cudaEventCreate", e));
+      }
     }
     std::string err;
-    rc = choose_dt(r.h, p.req.n, 0.0, p.req.cfl, p.req.dt_max, &r.dt, &err);
-    if (rc == SNS_OK) rc = capture_step(r.h, r.dt, &r.step, &err);
+    rc = choose_dt(r.slot.h, p.req.n, 0.0, p.req.cfl, p.req.dt_max, &r.dt, &err);
+    if (rc == SNS_OK) rc = capture_step(r.slot.h, r.dt, &r.step, &err);
     if (rc != SNS_OK) {
-      sns_destroy(r.h);
+      free_slot(r.slot);
       s->queue.pop_front();
       return server_fail(s, rc, "request " + std::to_string(p.id) + ": " + err);
     }
     s->queue.pop_front();
-    s->used += bytes;
+    s->used += r.slot.bytes;
     s->resident.push_back(r);
+  }
+  return SNS_OK;
+}
+
+// Has the older of the resident's in-flight batches completed?  Updates `pending`.
+int poll(sns_server* s, sns_server::Resident& r) {
+  while (r.pending > 0) {
+    const cudaEvent_t oldest = r.slot.ev[(r.head + 2 - r.pending) & 1];
+    const cudaError_t e = cudaEventQuery(oldest);
+    if (e == cudaErrorNotReady) return SNS_OK;
+    if (e != cudaSuccess) return server_fail(s, SNS_ERR_CUDA, cuda_msg("cudaEventQuery", e));
+    --r.pending;
   }
   return SNS_OK;
 }
@@ -374,7 +454,14 @@ int sns_server_create(size_t hbm_budget_bytes, int precision, sns_server** out) 
 int sns_server_destroy(sns_server* s) {
   if (s == nullptr) return SNS_ERR_INVALID;
   cudaSetDevice(s->device);
-  while (!s->resident.empty()) retire(s, s->resident.size() - 1);
+  while (!s->resident.empty()) {
+    sns_server::Resident& r = s->resident.back();
+    cudaStreamSynchronize(sns::handle_stream(r.slot.h));
+    if (r.step) cudaGraphExecDestroy(r.step);
+    free_slot(r.slot);
+    s->resident.pop_back();
+  }
+  for (sns_server::Slot& sl : s->idle) free_slot(sl);
   delete s;
   return SNS_OK;
 }
@@ -397,43 +484,53 @@ int sns_server_step(sns_server* s, sns_result* done, int max_done, int* ndone, i
   cudaSetDevice(s->device);
   int rc = admit(s);
   if (rc != SNS_OK) return rc;
-  // One tick: every resident solve advances on its own stream, the largest by one step and
-  // smaller ones by proportionally more (N_max^3 / N^3 steps, at most kMaxTickSteps), so a
-  // small solve is not held to the pace of the largest.  A full step replays the solve's
-  // graph; the last one (clipped to the horizon) is launched directly.
+  // Every resident solve with room in its two-batch window gets its next batch on its own
+  // stream: the largest by one step and smaller ones by proportionally more
+  // (N_max^3 / N^3 steps, at most kMaxTickSteps), so a small solve is not held to the pace
+  // of the largest.  A full step replays the solve's graph; the last one (clipped to the
+  // horizon) is launched directly.
   constexpr double kMaxTickSteps = 64.0;
   double wmax = 0.0;
   for (const sns_server::Resident& r : s->resident) wmax = std::fmax(wmax, std::pow((double)r.req.n, 3.0));
   for (sns_server::Resident& r : s->resident) {
+    rc = poll(s, r);
+    if (rc != SNS_OK) return rc;
+    if (r.pending >= 2 || r.t >= r.req.t_end - 1.0e-12 * r.req.t_end) continue;
+    cudaStream_t st = sns::handle_stream(r.slot.h);
     const int k = (int)std::fmin(kMaxTickSteps, std::fmax(1.0, std::floor(wmax / std::pow((double)r.req.n, 3.0))));
     for (int j = 0; j < k && r.t < r.req.t_end - 1.0e-12 * r.req.t_end; ++j) {
       const double left = r.req.t_end - r.t;
       if (left >= r.dt - 1.0e-14 * r.req.t_end) {
-        const cudaError_t e = cudaGraphLaunch(r.step, sns::handle_stream(r.h));
+        const cudaError_t e = cudaGraphLaunch(r.step, st);
         if (e != cudaSuccess) return server_fail(s, SNS_ERR_CUDA, cuda_msg("cudaGraphLaunch", e));
         r.t += r.dt;
       } else {
-        sns::enqueue_step(r.h, left);
+        sns::enqueue_step(r.slot.h, left);
         r.t = r.req.t_end;
       }
       ++r.steps;
     }
+    const cudaError_t e = cudaEventRecord(r.slot.ev[r.head], st);
+    if (e != cudaSuccess) return server_fail(s, SNS_ERR_CUDA, cuda_msg("cudaEventRecord", e));
+    r.head ^= 1;
+    ++r.pending;
   }
-  for (size_t i = 0; i < s->resident.size(); ++i) {
-    rc = sns::finish_handle(s->resident[i].h, "sns_server_step");
-    if (rc != SNS_OK) return server_fail(s, rc, sns::handle_error(s->resident[i].h));
-  }
-  // retire the solves that reached their horizon
+  // retire the solves whose last step has completed
   for (size_t i = s->resident.size(); i-- > 0;) {
     sns_server::Resident& r = s->resident[i];
     if (r.t < r.req.t_end - 1.0e-12 * r.req.t_end) continue;
+    rc = poll(s, r);
+    if (rc != SNS_OK) return rc;
+    if (r.pending > 0) continue;
+    rc = sns::finish_handle(r.slot.h, "sns_server_step");  // the device error word
+    if (rc != SNS_OK) return server_fail(s, rc, sns::handle_error(r.slot.h));
     sns_result res{};
     res.id = r.id;
     res.n = r.req.n;
     res.steps = r.steps;
     res.dt = r.dt;
-    rc = sns_diagnostics(r.h, r.req.t_end, &res.final);
-    if (rc != SNS_OK) return server_fail(s, rc, sns_last_error(r.h));
+    rc = sns_diagnostics(r.slot.h, r.req.t_end, &res.final);
+    if (rc != SNS_OK) return server_fail(s, rc, sns_last_error(r.slot.h));
     s->done.push_back(res);
     retire(s, i);
   }
@@ -446,6 +543,13 @@ int sns_server_step(sns_server* s, sns_result* done, int max_done, int* ndone, i
   if (resident) *resident = (int)s->resident.size();
   if (queued) *queued = (int)s->queue.size();
   if (bytes_in_use) *bytes_in_use = s->used;
+  return SNS_OK;
+}
+
+int sns_server_stats(const sns_server* s, size_t* idle_bytes, long long* handles_created) {
+  if (s == nullptr) return SNS_ERR_INVALID;
+  if (idle_bytes) *idle_bytes = s->idle_bytes;
+  if (handles_created) *handles_created = s->allocations;
   return SNS_OK;
 }
 

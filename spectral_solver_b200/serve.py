@@ -51,6 +51,7 @@ def run(stream, budget_bytes: int, precision: int, max_wall: float | None = None
     lat, finished, gpsteps = {}, {}, 0.0
     submitted = {}
     backlog_at_close = None
+    tick_s = []
     with Server(budget_bytes, precision) as srv:
         t0 = time.perf_counter()
         nxt = 0
@@ -64,7 +65,9 @@ def run(stream, budget_bytes: int, precision: int, max_wall: float | None = None
             if len(finished) == len(submitted):  # idle: wait for the next arrival
                 time.sleep(max(0.0, min(0.01, stream[nxt]["arrival"] - now)))
                 continue
+            ta = time.perf_counter()
             out, resident, queued, used = srv.step()
+            tick_s.append(time.perf_counter() - ta)
             done_at = time.perf_counter() - t0
             for res in out:
                 i = submitted[res["id"]]
@@ -76,6 +79,7 @@ def run(stream, budget_bytes: int, precision: int, max_wall: float | None = None
             if max_wall is not None and done_at > max_wall:
                 break
         wall = time.perf_counter() - t0
+        pool = srv.stats()
     lats = list(lat.values())
     offered = sum(r["n"] ** 3 * math.ceil(r["t_end"] / (0.5 * 2 * math.pi / r["n"])) for r in stream) / max(seconds, 1e-9)
     return {"precision": "fp64" if precision == PRECISION_FP64 else "fp32", "requests": len(stream),
@@ -85,7 +89,12 @@ def run(stream, budget_bytes: int, precision: int, max_wall: float | None = None
             "served_gpts_per_s": gpsteps / wall / 1e9 if wall > 0 else None,
             "offered_gpts_per_s_estimate": offered / 1e9,
             "backlog_when_arrivals_stop": backlog_at_close,
-            "drain_seconds": max(0.0, wall - seconds)}
+            "drain_seconds": max(0.0, wall - seconds),
+            # host time of a server tick (admission and re-initialisation of new solves,
+            # launches, retirement), which does not wait for GPU work
+            "tick_ms": {"p50": 1e3 * percentile(tick_s, 50), "p99": 1e3 * percentile(tick_s, 99),
+                        "max": 1e3 * max(tick_s)} if tick_s else None,
+            "handles_created": pool["handles_created"], "idle_pool_bytes_at_end": pool["idle_bytes"]}
 
 
 def main(argv=None):

@@ -127,3 +127,31 @@ def test_autotune_cache_and_parity(mod, tmp_path, n, precision):
     num = sum(float(np.sum(np.abs(x - y) ** 2)) for x, y in zip(r, r_ref))
     den = sum(float(np.sum(np.abs(y) ** 2)) for y in r_ref)
     assert math.sqrt(num / den) < (1e-12 if precision == FP64 else 2e-5)
+
+
+def test_server_reuses_retired_handles(mod):
+    """Retired solves leave their device memory in an idle pool and later requests of the
+    same N take it over: five 32^3 requests under a budget of two handles allocate two, and
+    each result is bitwise that of the request served alone by a fresh server."""
+    per = mod.load().sns_bytes_required(32, FP32)
+    reqs = [dict(n=32, nu=1 / (400.0 + 100 * i), t_end=0.3 + 0.1 * i, seed=20 + i, pert_amp=1e-3, pert_kmax=4)
+            for i in range(5)]
+    budget = int(per * 2.5)
+    done = {}
+    with mod.Server(budget, FP32) as srv:
+        ids = [srv.submit(**r) for r in reqs]
+        for _ in range(200000):
+            out, res, q, used = srv.step()
+            assert used <= budget
+            for r in out:
+                done[r["id"]] = r
+            if len(done) == len(reqs):
+                break
+        stats = srv.stats()
+    assert stats["handles_created"] == 2
+    assert stats["idle_bytes"] == 2 * per
+    for i, r in zip(ids, reqs):
+        alone, _ = run_server(mod, [r], budget)
+        assert done[i]["steps"] == alone[0]["steps"]
+        for key in ("kinetic_energy", "dissipation", "enstrophy", "max_velocity"):
+            assert done[i]["final"][key] == alone[0]["final"][key], key
