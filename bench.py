@@ -251,8 +251,8 @@ def workload_config(n: int, head: str, world: int) -> dict:
     same workload on the host cores)."""
     cb = 16 if head == "fp64" else 8
     pitch = ((n // 2 + 1) + 128 // cb - 1) // (128 // cb) * (128 // cb)
-    # 18 half fields, plus the FP32 form's compensation words of u (3 fields of 4 B per value)
-    resident = (18 * n * n * pitch * cb + (3 * n * n * pitch * 4 if head == "fp32" else 0)) / 1e9
+    # 18 half fields, plus the FP32 form's compensation words of u (3 fields of 2 B per value)
+    resident = (18 * n * n * pitch * cb + (3 * n * n * pitch * 2 if head == "fp32" else 0)) / 1e9
     return {"workload": f"Taylor-Green RK3 step, {n}^3, "
                         + ("FP32 precision form (mixed)" if head == "fp32" else "FP64 plain drop-in form")
                         + " (phase-shift dealiasing, sphere truncation, explicit viscosity)",

@@ -135,14 +135,15 @@ int sns_set_sphere_pruning(sns_handle* h, int enabled);
 
 /* Compensated state of the FP32 precision form (on by default there; no counterpart in the
  * reference, whose FP32 build rounds u to FP32 after every stage).  Each complex value of u
- * is kept as its FP32 value plus a bf16 pair holding the remainder, and the k-space sweep
- * forms the RK update u += b*dt*g and the projection of u in FP64 from the two.  Without it
- * the FP32 rounding of u drops the low bits of each stage's small increment, which over
- * thousands of steps dominates the form's error against FP64.  Costs 3 words per mode of
- * device memory and 6 words per mode of traffic in the sweep.  get_state returns the
- * compensated value and set_state fills both parts, so a state round-trips exactly.
- * Enabling it after it was off restarts the remainder at zero.  The FP64 form accepts 0
- * only (SNS_ERR_UNSUPPORTED for 1). */
+ * is kept as its FP32 value plus a 16-bit word holding the remainder of each part as an
+ * int8 multiple of 1/255 of its FP32 ulp, and the k-space sweep forms the RK update
+ * u += b*dt*g and the projection of u in FP64 from the two.  Without it the FP32 rounding of
+ * u drops the low bits of each stage's small increment, which over thousands of steps
+ * dominates the form's error against FP64.  Costs 3 words (6 bytes) per mode of device
+ * memory and 12 bytes per mode of traffic in the sweep.  get_state returns the compensated
+ * value and set_state fills both parts, so a state round-trips exactly.  Enabling it after
+ * it was off restarts the remainder at zero.  The FP64 form accepts 0 only
+ * (SNS_ERR_UNSUPPORTED for 1). */
 int sns_set_compensation(sns_handle* h, int enabled);
 
 /* Persistent grids chosen at creation: out[0] TMA y/z passes, out[1] two-stage x pass

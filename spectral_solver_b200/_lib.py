@@ -280,8 +280,9 @@ class Solver:
         self._check(self.lib.sns_set_sphere_pruning(self.h, 1 if enabled else 0))
 
     def set_compensation(self, enabled: bool):
-        """FP32 form: carry u as its FP32 value plus a bf16 remainder, the RK update formed in
-        FP64 (default on; the FP64 form accepts False only)."""
+        """FP32 form: carry u as its FP32 value plus an int8 remainder per part (1/255 of an
+        FP32 ulp), the RK update formed in FP64 (default on; the FP64 form accepts False
+        only)."""
         self._check(self.lib.sns_set_compensation(self.h, 1 if enabled else 0))
 
     def device_bytes(self) -> int:

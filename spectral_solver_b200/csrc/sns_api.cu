@@ -111,17 +111,17 @@ struct sns_handle {
   int nlive = 0;
   bool sphere_clean = false;
   bool prune = true;  // sns_set_sphere_pruning
-  // FP32 precision form: compensation words of u (3 fields of one 32-bit word per complex
+  // FP32 precision form: compensation words of u (3 fields of one 16-bit word per complex
   // value, the index of u), so the RK update keeps the low bits the FP32 state drops;
   // comp: in use (sns_set_compensation)
-  uint32_t* ulo = nullptr;
+  sns::CompWord* ulo = nullptr;
   bool comp = false;
   std::string err;
 
   char* u() const { return state; }
   char* gb() const { return state + 3 * fbytes; }
   char* ucomp(int c) const { return state + (size_t)c * fbytes; }
-  uint32_t* locomp(int c) const { return comp ? ulo + (size_t)c * g.field : nullptr; }
+  sns::CompWord* locomp(int c) const { return comp ? ulo + (size_t)c * g.field : nullptr; }
   char* wf(int i) const { return work + (size_t)i * fbytes; }
   int tcols() const { return ops->tile_cols; }
   int tiles_data() const { return (g.nh + tcols() - 1) / tcols(); }  // columns [0, N/2)
@@ -150,10 +150,10 @@ void upload_table(void* dst, const std::vector<double2>& t, int precision, cudaS
   }
 }
 
-// Bytes of the compensation words of u (FP32 form): 3 fields of 4 bytes per complex value.
+// Bytes of the compensation words of u (FP32 form): 3 fields of 2 bytes per complex value.
 size_t comp_bytes(int n, int precision) {
   if (precision != SNS_PRECISION_FP32) return 0;
-  return (size_t)3 * n * n * sns::pitch_for(n, 8) * sizeof(uint32_t);
+  return (size_t)3 * n * n * sns::pitch_for(n, 8) * sizeof(sns::CompWord);
 }
 
 size_t partial_slots(int n) {
@@ -467,14 +467,14 @@ bool nyquist_plane_dirty(int n, const double* full) {
 // Upload a reference full-layout field into half field `dst` (optionally Hermitian part).
 // The N^3 complex doubles of a full-layout field fit in work fields 4..11 for either precision.
 // With `lo` (FP32 form, compensated state) the remainder the FP32 value drops goes there.
-void upload_full(sns_handle* h, const double* host, void* dst, int herm, uint32_t* lo = nullptr) {
+void upload_full(sns_handle* h, const double* host, void* dst, int herm, sns::CompWord* lo = nullptr) {
   double2* staging = reinterpret_cast<double2*>(h->wf(4));
   const size_t bytes = (size_t)h->n * h->n * h->n * sizeof(double2);
   ck(cudaMemcpyAsync(staging, host, bytes, cudaMemcpyHostToDevice, h->stream), "upload");
   sns::launch_full_to_half(staging, dst, h->precision, herm, h->g, h->stream, lo);
 }
 
-void download_full(sns_handle* h, const void* src, double* host, const uint32_t* lo = nullptr) {
+void download_full(sns_handle* h, const void* src, double* host, const sns::CompWord* lo = nullptr) {
   double2* staging = reinterpret_cast<double2*>(h->wf(4));
   const size_t bytes = (size_t)h->n * h->n * h->n * sizeof(double2);
   sns::launch_half_to_full(src, h->precision, staging, h->g, h->stream, lo);

@@ -799,36 +799,44 @@ __device__ __forceinline__ C pair_value(C p0, C ps, C phase, bool keep, int deal
 // projection of u (:994-1039) -- or the RHS itself in modes 1 and 2.
 template <class C>
 __device__ __forceinline__ void finish_mode(C r[3], int ix, int iy, int iz, int n, C uu[3], C gg[3],
-                                            bool load_g, C rr[3], const SweepArgs& a, uint32_t lo[3]);
+                                            bool load_g, C rr[3], const SweepArgs& a, CompWord lo[3]);
 
 // Compensated state of the FP32 precision form.  The RK update u += b*dt*g adds an
 // increment some 1e-3 of |u| at dt = 1e-3; rounding u to FP32 after every stage drops the
 // increment's low bits, and over thousands of steps that dominates the form's error.  So u
-// is carried as its stored FP32 value hi plus a remainder lo, one 32-bit word per complex
-// value holding two bf16 (re in the low half, im in the high half).  The sweep forms the
-// update in FP64 from hi + lo.  lo is the remainder U - hi rounded toward zero (to FP32,
-// then to bf16 by dropping mantissa bits), so |lo| stays below half an FP32 ulp of hi and
-// round-to-nearest(hi + lo) gives hi back: the pair decodes to an FP64 value and encodes
-// back to the same pair (exact state round trips through the host).
-__device__ __forceinline__ double2 comp_decode(float2 hi, uint32_t lo) {
-  const float lr = __uint_as_float(lo << 16), li = __uint_as_float(lo & 0xffff0000u);
-  return make_double2((double)hi.x + (double)lr, (double)hi.y + (double)li);
+// is carried as its stored FP32 value hi plus a remainder, and the sweep forms the update
+// in FP64 from the two.  The remainder U - hi of each real part is kept as an int8 q, the
+// remainder in units of ulp(hi)/255 truncated toward zero (so |q| <= 127 and the decoded
+// value never reaches the rounding boundary of hi: round-to-nearest(hi + lo) == hi), and a
+// decoded pair encodes back to the same pair, so states round-trip exactly through the host.
+// The precision kept is about ulp(hi)/255, 2^-32 relative, against 2^-24 for FP32 alone.
+__device__ __forceinline__ double ulp_of(float hi) {  // 2^(E - 150), E the biased exponent (>= 1)
+  const int e = (int)((__float_as_uint(hi) >> 23) & 0xffu);
+  return __longlong_as_double((long long)((e > 0 ? e : 1) - 150 + 1023) << 52);
 }
-__device__ __forceinline__ float2 comp_encode(double2 U, uint32_t* lo) {
+__device__ __forceinline__ double comp_part(float hi, int q) { return ((double)q * ulp_of(hi)) / 255.0; }
+__device__ __forceinline__ int comp_q(double U, float hi) {
+  const double r = (U - (double)hi) / ulp_of(hi) * 255.0;  // U - hi exact; |r| <= 127.5
+  // toward zero, after a nudge of 1e-6 away from it: a decoded remainder (an integer up to
+  // FP64 round-off) comes back as the same integer, and the bounds 63.75 (hi a power of two,
+  // U below it) and 127.5 are never crossed
+  return (int)trunc(r + copysign(1.0e-6, r));
+}
+__device__ __forceinline__ double2 comp_decode(float2 hi, CompWord lo) {
+  const int qr = (int)(int8_t)(lo & 0xffu), qi = (int)(int8_t)(lo >> 8);
+  return make_double2((double)hi.x + comp_part(hi.x, qr), (double)hi.y + comp_part(hi.y, qi));
+}
+__device__ __forceinline__ float2 comp_encode(double2 U, CompWord* lo) {
   const float2 hi = make_float2(__double2float_rn(U.x), __double2float_rn(U.y));
-  // U - hi is exact in FP64 (the two are within a factor of two, or hi is zero)
-  const float lr = __double2float_rz(U.x - (double)hi.x), li = __double2float_rz(U.y - (double)hi.y);
-  uint32_t br = __float_as_uint(lr) & 0xffff0000u, bi = __float_as_uint(li) & 0xffff0000u;
-  if ((br & 0x7fffffffu) == 0u) br = 0u;  // no negative zeros: each value has one encoding
-  if ((bi & 0x7fffffffu) == 0u) bi = 0u;
-  *lo = (br >> 16) | bi;
+  const int qr = comp_q(U.x, hi.x), qi = comp_q(U.y, hi.y);
+  *lo = (CompWord)(((unsigned)(qr & 0xff)) | ((unsigned)(qi & 0xff) << 8));
   return hi;
 }
 
 template <class C>
 __device__ __forceinline__ void sweep_mode(const ModeIn<C>& in, int ix, int iy, int iz, int n, C phase,
                                            C uu[3], C gg[3], bool load_g, C rr[3],
-                                           const SweepArgs& a, uint32_t lo[3]) {
+                                           const SweepArgs& a, CompWord lo[3]) {
   const int m2 = ix * ix + iy * iy + iz * iz;
   const bool keep = 4LL * m2 <= (long long)n * n;
   const int kv[3] = {ix, iy, iz};
@@ -846,7 +854,7 @@ __device__ __forceinline__ void sweep_mode(const ModeIn<C>& in, int ix, int iy, 
 
 template <class C>
 __device__ __forceinline__ void finish_mode(C r[3], int ix, int iy, int iz, int n, C uu[3], C gg[3],
-                                            bool load_g, C rr[3], const SweepArgs& a, uint32_t lo[3]) {
+                                            bool load_g, C rr[3], const SweepArgs& a, CompWord lo[3]) {
   const int m2 = ix * ix + iy * iy + iz * iz;
   const bool keep = 4LL * m2 <= (long long)n * n;
   const double k2 = (double)m2;
@@ -905,7 +913,7 @@ __device__ __forceinline__ void finish_mode(C r[3], int ix, int iy, int iz, int 
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
           uu[c] = czero<C>();
-          lo[c] = 0u;
+          lo[c] = 0;
         }
       }
       return;
@@ -958,7 +966,7 @@ k_sweep(const C* __restrict__ work, C* __restrict__ u, C* __restrict__ gbuf,
       in.ps[p] = work[(long long)(2 * p + 1) * g.field + idx];
     }
     C uu[3], gg[3], rr[3];
-    uint32_t lo[3] = {0u, 0u, 0u};
+    CompWord lo[3] = {0, 0, 0};
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       uu[c] = u[(long long)c * g.field + idx];
@@ -1015,7 +1023,7 @@ k_sweep(const C* __restrict__ work, C* __restrict__ u, C* __restrict__ gbuf,
     }
     const long long idx = NH;
     C uu[3], gg[3], rr[3];
-    uint32_t lo[3] = {0u, 0u, 0u};
+    CompWord lo[3] = {0, 0, 0};
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       uu[c] = u[(long long)c * g.field + idx];
@@ -1067,7 +1075,7 @@ __global__ void __launch_bounds__(32) k_nyq_mode(C* __restrict__ u, C* __restric
     in.ps[p] = cmk((real_of<C>)part[2 * p + 1], real_of<C>(0));
   }
   C uu[3], gg[3], rr[3];
-  uint32_t lo[3] = {0u, 0u, 0u};
+  CompWord lo[3] = {0, 0, 0};
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
     uu[c] = u[(long long)c * g.field + NH];
@@ -1191,7 +1199,7 @@ k_sweep_rot(const C* __restrict__ work, C* __restrict__ u, C* __restrict__ gbuf,
     const int m2 = mx * mx + my * my + mz * mz;
     const bool keep = 4LL * m2 <= (long long)N * N;
     C r[3], uu[3], gg[3], rr[3];
-    uint32_t lo[3] = {0u, 0u, 0u};
+    CompWord lo[3] = {0, 0, 0};
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       r[c] = pair_value(A[c], B[c], ph, keep, a.dealias);
@@ -1413,8 +1421,8 @@ k_p5(const __grid_constant__ CUtensorMap map, C* __restrict__ u, C* __restrict__
       // Two-deep software pipeline over this thread's modes: the u, g loads of mode q + 1
       // are in flight while mode q is combined and stored (different modes, no aliasing).
       C uu_n[3], gg_n[3];
-      uint32_t lo_n[3] = {0u, 0u, 0u};
-      auto load_mode = [&](int q, C* uu, C* gg, uint32_t* lo) {
+      CompWord lo_n[3] = {0, 0, 0};
+      auto load_mode = [&](int q, C* uu, C* gg, CompWord* lo) {
         const long long idx = ((long long)mode_e(q) * N + my) * g.pitch + mx0 + mode_s(q);
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
@@ -1427,7 +1435,7 @@ k_p5(const __grid_constant__ CUtensorMap map, C* __restrict__ u, C* __restrict__
 #pragma unroll 1
       for (int q = 0; q < MPT; ++q) {
         C uu[3], gg[3], rr[3];
-        uint32_t lo[3];
+        CompWord lo[3];
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
           uu[c] = uu_n[c];
@@ -1644,7 +1652,7 @@ __device__ __forceinline__ double2 widen(double2 v) { return v; }
 __device__ __forceinline__ double2 widen(float2 v) { return make_double2(v.x, v.y); }
 
 template <class C>
-__device__ __forceinline__ double2 widen_comp(const C* half, const uint32_t* lo, long long i) {
+__device__ __forceinline__ double2 widen_comp(const C* half, const CompWord* lo, long long i) {
   if constexpr (sizeof(C) == 8) {
     if (lo) return comp_decode(half[i], lo[i]);
   }
@@ -1653,7 +1661,7 @@ __device__ __forceinline__ double2 widen_comp(const C* half, const uint32_t* lo,
 
 template <class C>
 __global__ void k_half_to_full(const C* __restrict__ half, double2* __restrict__ full, Geom g,
-                               const uint32_t* __restrict__ lo) {
+                               const CompWord* __restrict__ lo) {
   const long long n = g.n;
   const long long total = n * n * n;
   const long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -1672,7 +1680,7 @@ __global__ void k_half_to_full(const C* __restrict__ half, double2* __restrict__
 // (c_m + conj(c_-m))/2 is stored, so a c2r of the result equals Re(IDFT(c)).
 template <class C>
 __global__ void k_full_to_half(const double2* __restrict__ full, C* __restrict__ half, int hermitian_part,
-                               Geom g, uint32_t* __restrict__ lo) {
+                               Geom g, CompWord* __restrict__ lo) {
   const long long n = g.n;
   const long long total = n * n * (g.nh + 1);
   const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -2042,14 +2050,14 @@ void launch_add_sparse(void* u, int precision, const long long* idx, const doubl
   else k_add_sparse<float2><<<blocks_for(count, 256), 256, 0, st>>>(FC<float2>(u), idx, val, count);
 }
 void launch_half_to_full(const void* half, int precision, double2* full, Geom g, cudaStream_t st,
-                         const uint32_t* lo) {
+                         const CompWord* lo) {
   const long long total = (long long)g.n * g.n * g.n;
   if (precision == 0)
     k_half_to_full<double2><<<blocks_for(total, 256), 256, 0, st>>>(FC<double2>(half), full, g, nullptr);
   else k_half_to_full<float2><<<blocks_for(total, 256), 256, 0, st>>>(FC<float2>(half), full, g, lo);
 }
 void launch_full_to_half(const double2* full, void* half, int precision, int hermitian_part, Geom g,
-                         cudaStream_t st, uint32_t* lo) {
+                         cudaStream_t st, CompWord* lo) {
   const long long total = (long long)g.n * g.n * (g.nh + 1);
   if (precision == 0)
     k_full_to_half<double2><<<blocks_for(total, 256), 256, 0, st>>>(full, FC<double2>(half), hermitian_part, g,

@@ -26,6 +26,11 @@ __host__ __device__ inline int pitch_for(int n, int complex_bytes) {
 }
 __host__ __device__ inline int pitch_for(int n) { return pitch_for(n, 16); }
 
+// Compensation word of one complex value of u in the FP32 precision form: the remainder of
+// the real and imaginary parts as signed multiples of 1/255 of their FP32 ulp (int8 each,
+// real part in the low byte).
+using CompWord = uint16_t;
+
 // Per-stage scalars of the fused k-space sweep (the reference's Real-typed RK products,
 // ava_taylor_green_impl.hpp:998, 1014, 1030).
 struct SweepArgs {
@@ -38,9 +43,9 @@ struct SweepArgs {
   int dealias;     // 1: phase-shift pair, 0: plain product only
   int visc_if;     // 0: explicit viscous term in the RHS (the reference); 1: integrating factor
   // FP32 precision form, compensated state: one word per complex value of u (same index as
-  // u; a bf16 pair, re in the low half) holding the part of the FP64 update that the FP32
-  // value cannot; null: u is the FP32 value alone (and always in the FP64 form)
-  uint32_t* ulo;
+  // u) holding the part of the FP64 update that the FP32 value cannot; null: u is the FP32
+  // value alone (and always in the FP64 form)
+  CompWord* ulo;
 };
 
 // Arguments of the TMA-fed streaming y/z pass.
@@ -121,9 +126,9 @@ void launch_add_sparse(void* u, int precision, const long long* idx, const doubl
 // `lo` (FP32 form, may be null): the compensation words of the half field (see SweepArgs::ulo);
 // half_to_full adds them, full_to_half writes the remainder the FP32 value drops
 void launch_half_to_full(const void* half, int precision, double2* full, Geom g, cudaStream_t st,
-                         const uint32_t* lo = nullptr);
+                         const CompWord* lo = nullptr);
 void launch_full_to_half(const double2* full, void* half, int precision, int hermitian_part, Geom g,
-                         cudaStream_t st, uint32_t* lo = nullptr);
+                         cudaStream_t st, CompWord* lo = nullptr);
 void launch_spectral_diag(const void* u, int precision, double* partials, int nblocks, Geom g, cudaStream_t st);
 void launch_reduce(const double* partials, int count, int stride, int op_max, double* out, cudaStream_t st);
 

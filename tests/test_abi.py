@@ -34,8 +34,8 @@ def test_version_and_sizes(lib):
     assert 18e9 < b512 < 22e9  # 18 half-spectrum fields at 512^3
     b512f = lib.sns_bytes_required(512, 1)
     # the same 18 fields in FP32 (rows padded to 16 complex floats) plus the compensation
-    # words of u (3 fields of 4 bytes per complex value)
-    assert 10.5e9 < b512f < 12e9
+    # words of u (3 fields of 2 bytes per complex value)
+    assert 10.4e9 < b512f < 11.2e9
     assert lib.sns_bytes_required(0, 0) == 0
     assert lib.sns_bytes_required(64, 7) == 0
 
