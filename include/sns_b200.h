@@ -106,6 +106,19 @@ int sns_nonlinear(sns_handle* h, const double* const uhat_full[3], double* const
 /* nsteps Williamson RK3 steps of size dt (TaylorGreenSolver::step_rk3, :979-1045). */
 int sns_step(sns_handle* h, double dt, int nsteps);
 
+/* Adaptive CFL stepping on the device (the reference's rule of run_taylor_green,
+ * ava_taylor_green_impl.hpp:1363-1378, dt = min(dt_max, cfl * (2 pi / N) / vmax) clipped to
+ * the horizon, evaluated before every step from the current state's vmax).  sns_set_clock
+ * starts the handle's clock at t with horizon t_end (INFINITY: none); each sns_step_cfl step
+ * computes vmax, the step size and the new time on the device (nothing waits for the host,
+ * so batches and servers replay it from graphs) and stops the clock at the horizon, after
+ * which a step leaves the state as it is.  sns_get_clock writes {t, last step size, steps
+ * taken, stopped (0/1)}.  The steps equal, bit for bit, those of the host loop that calls
+ * sns_max_velocity and sns_step with the same rule. */
+int sns_set_clock(sns_handle* h, double t, double t_end, double cfl, double dt_max);
+int sns_step_cfl(sns_handle* h, int nsteps);
+int sns_get_clock(sns_handle* h, double* out, int count);
+
 /* Diagnostics of the current state (TaylorGreenSolver::diagnostics, :1122-1179) and the
  * maximum velocity magnitude (TaylorGreenSolver::max_velocity, :1105-1120). */
 int sns_diagnostics(sns_handle* h, double t, sns_diag* out);
@@ -184,7 +197,8 @@ typedef struct sns_solve_spec {
   uint64_t seed;     /* perturbation seed */
   double pert_amp;   /* perturbation rms amplitude (0: pure Taylor-Green) */
   int pert_kmax;     /* perturbation shell 1 <= |m| <= pert_kmax */
-  double dt;         /* > 0: fixed time step; <= 0: CFL-limited from the initial field */
+  double dt;         /* > 0: fixed time step; <= 0: the CFL step, recomputed on the device before
+                        every step from the current vmax (sns_step_cfl; no horizon) */
   double cfl;        /* CFL number for dt <= 0 (dt = min(dt_max, cfl * (2 pi / N) / vmax)) */
   double dt_max;     /* cap of the CFL step */
 } sns_solve_spec;
@@ -192,7 +206,8 @@ typedef struct sns_solve_spec {
 /* Create `count` solves and capture the batch step graph.  With autotune_trials > 0 the
  * launch shape of each distinct (N, precision) is chosen by sns_autotune on a scratch handle
  * (cached in autotune_cache when non-NULL) and used by every solve of that key.  out_dt
- * (may be NULL) receives each solve's time step. */
+ * (may be NULL) receives each solve's fixed step, or the first step of a CFL solve (its
+ * later steps follow its vmax; sns_get_clock on sns_batch_handle(b, i) reads them). */
 int sns_batch_create(const sns_solve_spec* specs, int count, int autotune_trials, const char* autotune_cache,
                      sns_batch** out, double* out_dt);
 int sns_batch_destroy(sns_batch* b);
@@ -227,8 +242,9 @@ int sns_autotune(sns_handle* h, int trial_steps, const char* cache_path, int* ou
  * is kept in an idle pool and the next request of the same N re-initialises it in place, so
  * a steady stream admits and retires without cudaMalloc / cudaFree; the budget counts
  * resident and idle memory, and idle handles of another N are freed only to make room.
- * Each solve's step is fixed at admission by the CFL rule on its initial field; each result
- * is bitwise that of the same request solved alone. */
+ * Every step of a solve is the reference's adaptive CFL step, computed on the device from
+ * the solve's current vmax and clipped to its horizon (sns_step_cfl); each result is bitwise
+ * that of the same request solved alone. */
 typedef struct sns_server sns_server;
 
 typedef struct sns_request {
@@ -238,15 +254,15 @@ typedef struct sns_request {
   uint64_t seed;     /* perturbation seed */
   double pert_amp;   /* perturbation rms amplitude */
   int pert_kmax;     /* perturbation shell */
-  double cfl;        /* CFL number of the fixed step chosen at admission */
-  double dt_max;     /* cap of that step */
+  double cfl;        /* CFL number of every step */
+  double dt_max;     /* cap of the step */
 } sns_request;
 
 typedef struct sns_result {
   int64_t id;        /* id returned by sns_server_submit */
   int n;
   int steps;         /* RK3 steps taken (the last one clipped to t_end) */
-  double dt;         /* the solve's step */
+  double dt;         /* the mean step, t_end / steps */
   sns_diag final;    /* diagnostics at t_end */
 } sns_result;
 

@@ -99,6 +99,9 @@ SIGNATURES = {
                                   C.POINTER(C.c_int), C.POINTER(C.c_size_t)]),
     "sns_server_last_error": (C.c_char_p, [C.c_void_p]),
     "sns_grid_supported": (C.c_int, [C.c_int]),
+    "sns_set_clock": (C.c_int, [_H, C.c_double, C.c_double, C.c_double, C.c_double]),
+    "sns_step_cfl": (C.c_int, [_H, C.c_int]),
+    "sns_get_clock": (C.c_int, [_H, _DP, C.c_int]),
     "sns_server_stats": (C.c_int, [C.c_void_p, C.POINTER(C.c_size_t), C.POINTER(C.c_longlong)]),
     "sns_fft3d_create": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
                                    C.POINTER(C.c_void_p)]),
@@ -239,6 +242,19 @@ class Solver:
         self._check(self.lib.sns_step(self.h, dt, nsteps))
 
     step_rk3 = step
+
+    def set_clock(self, t: float = 0.0, t_end: float = float("inf"), cfl: float = 0.5, dt_max: float = 0.5):
+        """Start the device clock for adaptive CFL steps (sns_step_cfl)."""
+        self._check(self.lib.sns_set_clock(self.h, t, t_end, cfl, dt_max))
+
+    def step_cfl(self, nsteps: int = 1):
+        """nsteps adaptive CFL steps taken on the device (no-ops once the horizon is reached)."""
+        self._check(self.lib.sns_step_cfl(self.h, nsteps))
+
+    def clock(self) -> dict:
+        out = (C.c_double * 4)()
+        self._check(self.lib.sns_get_clock(self.h, out, 4))
+        return {"t": out[0], "dt": out[1], "steps": int(out[2]), "stopped": bool(out[3])}
 
     def time_steps(self, dt: float, nsteps: int) -> float:
         ms = C.c_double()

@@ -85,6 +85,8 @@ struct sns_handle {
   double* partials = nullptr;
   double* red = nullptr;  // reduction results
   int* err_word = nullptr;  // device error word written by bounded waits
+  double* clock = nullptr;  // device clock of adaptive-CFL stepping (sns::kClock* slots)
+  bool on_clock = false;    // the stages being enqueued take their step from the clock
   int tma_grid = 0;         // persistent CTAs of the TMA passes
   int x2_grid = 0;          // persistent CTAs of the two-stage x pass (0: generic x pass)
   int p5_grid = 0;          // persistent CTAs of the fused forward-z + sweep pass (0: two kernels)
@@ -332,6 +334,8 @@ sns::SweepArgs stage_args(const sns_handle* h, int stage, double dt, int mode, c
   a.nu = h->nu;
   // the compensated update applies to the handle's own state only (not to sns_rhs inputs)
   a.ulo = (h->comp && mode == 0 && u_src == h->u()) ? h->ulo : nullptr;
+  // adaptive stepping: the step size comes from the device clock
+  a.clock = (h->on_clock && mode == 0) ? h->clock : nullptr;
   a.stage = stage;
   a.mode = mode;
   a.dealias = 1;
@@ -452,6 +456,24 @@ void step_once(sns_handle* h, double dt) {
   }
 }
 
+void velocity_reductions(sns_handle* h);
+
+// One step with the adaptive CFL rule on the device: vmax of the current state (the same
+// reductions as sns_max_velocity), the clock's next step from it, then the three stages on
+// that step.  Nothing here waits for the host, so the step can be captured into a graph.
+void step_on_clock(sns_handle* h) {
+  velocity_reductions(h);
+  sns::launch_clock_step(h->red + 1, h->clock, h->stream);
+  h->on_clock = true;
+  try {
+    step_once(h, 0.0);
+  } catch (...) {
+    h->on_clock = false;
+    throw;
+  }
+  h->on_clock = false;
+}
+
 // Does a reference full-layout spectrum carry content on the plane mx = N/2 off (N/2,0,0)?
 bool nyquist_plane_dirty(int n, const double* full) {
   const int nh = n / 2;
@@ -561,6 +583,7 @@ void release(sns_handle* h) {
   cudaFree(h->partials);
   cudaFree(h->red);
   cudaFree(h->err_word);
+  cudaFree(h->clock);
   cudaFree(h->tw2);
   cudaFree(h->nyq_part);
   cudaFree(h->xf);
@@ -578,6 +601,8 @@ namespace sns {
 
 // Hooks for the batch and serving layers in this library (not part of the C ABI).
 void enqueue_step(sns_handle* h, double dt) { step_once(h, dt); }
+void enqueue_clock_step(sns_handle* h) { step_on_clock(h); }
+double* handle_clock(sns_handle* h) { return h->clock; }
 cudaStream_t handle_stream(const sns_handle* h) { return h->stream; }
 int handle_device(const sns_handle* h) { return h->device; }
 // Synchronise the handle's stream and check its device error word; SNS code, message in h.
@@ -634,7 +659,8 @@ int sns_grid_supported(int n) { return n > 0 && sns::ops_for(n, 0) != nullptr ? 
 size_t sns_bytes_required(int n, int precision) {
   if (n <= 0 || (precision != SNS_PRECISION_FP64 && precision != SNS_PRECISION_FP32)) return 0;
   return 18 * field_bytes(n, precision) + comp_bytes(n, precision) + partial_slots(n) * sizeof(double) +
-         (size_t)(4 * n + 64) * complex_bytes(precision) + (size_t)n * (n / 16 + 1) * sizeof(int);
+         (size_t)(4 * n + 64) * complex_bytes(precision) + (size_t)n * (n / 16 + 1) * sizeof(int) +
+         sns::kClockWords * sizeof(double);
 }
 
 int sns_create(int n, double nu, int precision, int viscous_mode, uint64_t seed, double pert_amp, int pert_kmax,
@@ -718,6 +744,8 @@ int sns_create(int n, double nu, int precision, int viscous_mode, uint64_t seed,
     alloc((void**)&h->partials, h->partial_count * sizeof(double));
     alloc((void**)&h->red, 16 * sizeof(double));
     alloc((void**)&h->err_word, sizeof(int));
+    alloc((void**)&h->clock, sns::kClockWords * sizeof(double));
+    ck(cudaMemsetAsync(h->clock, 0, sns::kClockWords * sizeof(double), h->stream), "memset");
     ck(cudaMemsetAsync(h->err_word, 0, sizeof(int), h->stream), "memset");
     int nsm = 0;
     ck(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device), "cudaDeviceGetAttribute");
@@ -940,6 +968,42 @@ int sns_autotune(sns_handle* h, int trial_steps, const char* cache_path, int* ou
       out_config[1] = h->x2_grid;
       out_config[2] = h->p5_grid;
     }
+  });
+}
+
+int sns_set_clock(sns_handle* h, double t, double t_end, double cfl, double dt_max) {
+  return guarded(h, [&] {
+    if (!std::isfinite(t) || !(t_end > t) || !(cfl > 0.0) || !(dt_max > 0.0))
+      throw SnsError(SNS_ERR_INVALID, "the clock needs t finite, t_end > t (INFINITY allowed), cfl > 0, dt_max > 0");
+    double c[sns::kClockWords] = {};
+    c[sns::kClockT] = t;
+    c[sns::kClockTEnd] = t_end;
+    c[sns::kClockCfl] = cfl;
+    c[sns::kClockDtMax] = dt_max;
+    c[sns::kClockDx] = 2.0 * kPi / static_cast<double>(h->n);
+    ck(cudaMemcpyAsync(h->clock, c, sizeof c, cudaMemcpyHostToDevice, h->stream), "clock");
+    sync(h, "sns_set_clock");
+  });
+}
+
+int sns_step_cfl(sns_handle* h, int nsteps) {
+  return guarded(h, [&] {
+    if (nsteps < 0) throw SnsError(SNS_ERR_INVALID, "negative step count");
+    for (int k = 0; k < nsteps; ++k) step_on_clock(h);
+    sync(h, "sns_step_cfl");
+  });
+}
+
+int sns_get_clock(sns_handle* h, double* out, int count) {
+  return guarded(h, [&] {
+    if (out == nullptr || count < 4) throw SnsError(SNS_ERR_INVALID, "out needs 4 doubles");
+    double c[sns::kClockWords];
+    ck(cudaMemcpyAsync(c, h->clock, sizeof c, cudaMemcpyDeviceToHost, h->stream), "clock");
+    sync(h, "sns_get_clock");
+    out[0] = c[sns::kClockT];
+    out[1] = c[sns::kClockDt];
+    out[2] = c[sns::kClockSteps];
+    out[3] = c[sns::kClockStopped];
   });
 }
 

@@ -810,13 +810,18 @@ __device__ __forceinline__ void finish_mode(C r[3], int ix, int iy, int iz, int 
 // value never reaches the rounding boundary of hi: round-to-nearest(hi + lo) == hi), and a
 // decoded pair encodes back to the same pair, so states round-trip exactly through the host.
 // The precision kept is about ulp(hi)/255, 2^-32 relative, against 2^-24 for FP32 alone.
-__device__ __forceinline__ double ulp_of(float hi) {  // 2^(E - 150), E the biased exponent (>= 1)
+// ulp(hi) = 2^(E - 150) and its inverse, E the biased exponent of hi (at least 1), built from
+// the exponent bits: no division anywhere in the encoding.
+__device__ __forceinline__ int comp_exp(float hi) {
   const int e = (int)((__float_as_uint(hi) >> 23) & 0xffu);
-  return __longlong_as_double((long long)((e > 0 ? e : 1) - 150 + 1023) << 52);
+  return e > 0 ? e : 1;
 }
-__device__ __forceinline__ double comp_part(float hi, int q) { return ((double)q * ulp_of(hi)) / 255.0; }
+__device__ __forceinline__ double pow2(int k) { return __longlong_as_double((long long)(k + 1023) << 52); }
+__device__ __forceinline__ double comp_part(float hi, int q) {
+  return (double)q * pow2(comp_exp(hi) - 150) * (1.0 / 255.0);
+}
 __device__ __forceinline__ int comp_q(double U, float hi) {
-  const double r = (U - (double)hi) / ulp_of(hi) * 255.0;  // U - hi exact; |r| <= 127.5
+  const double r = (U - (double)hi) * pow2(150 - comp_exp(hi)) * 255.0;  // U - hi exact; |r| <= 127.5
   // toward zero, after a nudge of 1e-6 away from it: a decoded remainder (an integer up to
   // FP64 round-off) comes back as the same integer, and the bounds 63.75 (hi a power of two,
   // U below it) and 127.5 are never crossed
@@ -831,6 +836,26 @@ __device__ __forceinline__ float2 comp_encode(double2 U, CompWord* lo) {
   const int qr = comp_q(U.x, hi.x), qi = comp_q(U.y, hi.y);
   *lo = (CompWord)(((unsigned)(qr & 0xff)) | ((unsigned)(qi & 0xff) << 8));
   return hi;
+}
+
+// Per-stage scalars with the step taken from a device clock: the same expressions as the
+// host's stage arguments (the reference's Real-typed products, :998, 1014, 1030), on the
+// clock's current step size.
+__device__ __forceinline__ SweepArgs resolve_step(SweepArgs a) {
+  if (a.clock == nullptr) return a;
+  const double dt = a.clock[kClockDt];
+  a.frozen = a.clock[kClockStopped] != 0.0;
+  if (a.stage == 0) {
+    a.ub = dt / 3.0;
+    a.if_tau = dt / 3.0;
+  } else if (a.stage == 1) {
+    a.ub = 15.0 * dt / 16.0;
+    a.if_tau = 5.0 * dt / 12.0;
+  } else {
+    a.ub = 8.0 * dt / 15.0;
+    a.if_tau = dt / 4.0;
+  }
+  return a;
 }
 
 template <class C>
@@ -883,6 +908,7 @@ __device__ __forceinline__ void finish_mode(C r[3], int ix, int iy, int iz, int 
     rr[2] = r[2];
     return;
   }
+  if (a.frozen) return;  // the solve's clock reached its horizon: u and g stay as they are
   if constexpr (sizeof(C) == 8) {
     if (a.ulo != nullptr) {
       // FP32 form with the compensated state: u = hi + lo updated and projected in FP64
@@ -948,7 +974,8 @@ template <int N, class C>
 __global__ void __launch_bounds__(256)
 k_sweep(const C* __restrict__ work, C* __restrict__ u, C* __restrict__ gbuf,
         C* __restrict__ rhs, const double* __restrict__ nyq_part, int nparts, const C* __restrict__ phase,
-        SweepArgs a, Geom g) {
+        SweepArgs a0, Geom g) {
+  const SweepArgs a = resolve_step(a0);
   constexpr int NH = N / 2;
   const long long e = (long long)blockIdx.x * 256 + threadIdx.x;
   const long long total = (long long)N * N * NH;
@@ -1054,7 +1081,8 @@ k_sweep(const C* __restrict__ work, C* __restrict__ u, C* __restrict__ gbuf,
 template <int N, class C>
 __global__ void __launch_bounds__(32) k_nyq_mode(C* __restrict__ u, C* __restrict__ gbuf,
                                                  C* __restrict__ rhs, const double* __restrict__ nyq_part,
-                                                 int nparts, const C* __restrict__ phase, SweepArgs a, Geom g) {
+                                                 int nparts, const C* __restrict__ phase, SweepArgs a0, Geom g) {
+  const SweepArgs a = resolve_step(a0);
   constexpr int NH = N / 2;
   const int tid = threadIdx.x;
   const bool load_g = a.stage > 0;
@@ -1189,7 +1217,8 @@ k_xpass_rot(C* __restrict__ work, const C* __restrict__ unyq, const C* __restric
 template <int N, class C>
 __global__ void __launch_bounds__(256)
 k_sweep_rot(const C* __restrict__ work, C* __restrict__ u, C* __restrict__ gbuf, C* __restrict__ rhs,
-            const double* __restrict__ nyq_sums, const C* __restrict__ phase, SweepArgs a, Geom g) {
+            const double* __restrict__ nyq_sums, const C* __restrict__ phase, SweepArgs a0, Geom g) {
+  const SweepArgs a = resolve_step(a0);
   constexpr int NH = N / 2;
   const long long e = (long long)blockIdx.x * 256 + threadIdx.x;
   const long long total = (long long)N * N * NH;
@@ -1277,8 +1306,9 @@ template <int N, class C>
 __global__ void __launch_bounds__(nt_p5<N>(), tma_minb<N>())
 k_p5(const __grid_constant__ CUtensorMap map, C* __restrict__ u, C* __restrict__ gbuf,
      C* __restrict__ rhs, const double* __restrict__ nyq_part, int nparts, const C* __restrict__ tw,
-     const C* __restrict__ phase, SweepArgs a, int ncb, const int* __restrict__ live, int nlive, Geom g,
+     const C* __restrict__ phase, SweepArgs a0, int ncb, const int* __restrict__ live, int nlive, Geom g,
      int* err) {
+  const SweepArgs a = resolve_step(a0);
   constexpr int NT = nt_p5<N>();
   constexpr int BR = box_rows<N>();
   constexpr int NBOX = N / BR;
@@ -2069,6 +2099,29 @@ void launch_spectral_diag(const void* u, int precision, double* partials, int nb
   if (precision == 0) k_spectral_diag<double2><<<nblocks, 256, 0, st>>>(FC<double2>(u), partials, g);
   else k_spectral_diag<float2><<<nblocks, 256, 0, st>>>(FC<float2>(u), partials, g);
 }
+// One thread: the reference's adaptive step (run_taylor_green, ava_taylor_green_impl.hpp:
+// 1363-1378) on the device, with the horizon in place of the output times.
+__global__ void k_clock_step(const double* __restrict__ vmax2, double* __restrict__ c) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const double t = c[kClockT], t_end = c[kClockTEnd];
+  if (c[kClockStopped] != 0.0 || !(t < t_end - 1.0e-14)) {
+    c[kClockStopped] = 1.0;
+    c[kClockDt] = 0.0;
+    return;
+  }
+  const double vmax = sqrt(*vmax2);
+  double main_dt = c[kClockDtMax];
+  if (vmax > 1.0e-14) main_dt = fmin(main_dt, c[kClockCfl] * c[kClockDx] / vmax);
+  const double dt = fmin(main_dt, t_end - t);
+  c[kClockDt] = dt;
+  c[kClockT] = t + dt;
+  c[kClockSteps] += 1.0;
+}
+
+void launch_clock_step(const double* vmax2, double* clock, cudaStream_t st) {
+  k_clock_step<<<1, 32, 0, st>>>(vmax2, clock);
+}
+
 void launch_reduce(const double* partials, int count, int stride, int op_max, double* out, cudaStream_t st) {
   k_reduce<<<1, 256, 0, st>>>(partials, count, stride, op_max, out);
 }

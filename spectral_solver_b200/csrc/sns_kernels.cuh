@@ -46,7 +46,17 @@ struct SweepArgs {
   // u) holding the part of the FP64 update that the FP32 value cannot; null: u is the FP32
   // value alone (and always in the FP64 form)
   CompWord* ulo;
+  // Step taken on the device (adaptive CFL): null, or the handle's clock (kClock* slots),
+  // whose current step size replaces the host's dt in ub and if_tau; when the clock is
+  // stopped (its horizon reached) the stage leaves u and g as they are
+  const double* clock;
+  int frozen;  // set in the kernel from the clock
 };
+
+// Device clock of a solve stepped with an adaptive CFL step (doubles): the step size of the
+// current step, time, horizon, CFL number, step cap, grid spacing, steps taken, stopped flag.
+enum { kClockDt = 0, kClockT, kClockTEnd, kClockCfl, kClockDtMax, kClockDx, kClockSteps, kClockStopped,
+       kClockWords = 8 };
 
 // Arguments of the TMA-fed streaming y/z pass.
 struct TmaArgs {
@@ -131,6 +141,10 @@ void launch_full_to_half(const double2* full, void* half, int precision, int her
                          cudaStream_t st, CompWord* lo = nullptr);
 void launch_spectral_diag(const void* u, int precision, double* partials, int nblocks, Geom g, cudaStream_t st);
 void launch_reduce(const double* partials, int count, int stride, int op_max, double* out, cudaStream_t st);
+// The next step of a device clock from vmax^2 (the reference's adaptive rule,
+// ava_taylor_green_impl.hpp:1363-1368): dt = min(dt_max, cfl dx / vmax), clipped to the
+// horizon; stops the clock at the horizon; advances t and the step count.
+void launch_clock_step(const double* vmax2, double* clock, cudaStream_t st);
 
 }  // namespace sns
 
@@ -140,6 +154,8 @@ namespace sns {
 
 // Handle hooks for the batch and serving layers (defined in sns_api.cu).
 void enqueue_step(sns_handle* h, double dt);  // one RK3 step on the handle's stream, no sync
+void enqueue_clock_step(sns_handle* h);       // one adaptive-CFL step on the device clock, no sync
+double* handle_clock(sns_handle* h);
 cudaStream_t handle_stream(const sns_handle* h);
 int handle_device(const sns_handle* h);
 int finish_handle(sns_handle* h, const char* what);  // sync + device error word -> SNS code

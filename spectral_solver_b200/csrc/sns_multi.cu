@@ -49,37 +49,14 @@ int choose_dt(sns_handle* h, int n, double dt, double cfl, double dt_max, double
   return SNS_OK;
 }
 
-// One RK3 step of `h` with step dt captured into an executable graph on the handle's stream.
-int capture_step(sns_handle* h, double dt, cudaGraphExec_t* exec, std::string* err) {
-  cudaStream_t st = sns::handle_stream(h);
-  cudaGraph_t graph = nullptr;
-  cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
-  if (e != cudaSuccess) {
-    *err = cuda_msg("cudaStreamBeginCapture", e);
-    return SNS_ERR_CUDA;
-  }
-  sns::enqueue_step(h, dt);
-  e = cudaStreamEndCapture(st, &graph);
-  if (e != cudaSuccess) {
-    *err = cuda_msg("cudaStreamEndCapture", e);
-    return SNS_ERR_CUDA;
-  }
-  e = cudaGraphInstantiate(exec, graph, 0);
-  cudaGraphDestroy(graph);
-  if (e != cudaSuccess) {
-    *err = cuda_msg("cudaGraphInstantiate", e);
-    return SNS_ERR_CUDA;
-  }
-  return SNS_OK;
-}
-
 }  // namespace
 
 // ---------------------------------------------------------------------------------------
 // Batched ensemble.
 struct sns_batch {
   std::vector<sns_handle*> h;
-  std::vector<double> dt;
+  std::vector<double> dt;      // fixed step, or the first CFL step of an adaptive member
+  std::vector<char> adaptive;  // the member takes a CFL step from its device clock every step
   std::vector<cudaEvent_t> join;
   cudaStream_t origin = nullptr;
   cudaEvent_t fork = nullptr, ev0 = nullptr, ev1 = nullptr;
@@ -122,7 +99,8 @@ int batch_capture(sns_batch* b) {
     cudaStream_t st = sns::handle_stream(b->h[i]);
     e = cudaStreamWaitEvent(st, b->fork, 0);
     if (e != cudaSuccess) break;
-    sns::enqueue_step(b->h[i], b->dt[i]);
+    if (b->adaptive[i]) sns::enqueue_clock_step(b->h[i]);
+    else sns::enqueue_step(b->h[i], b->dt[i]);
     e = cudaEventRecord(b->join[i], st);
     if (e == cudaSuccess) e = cudaStreamWaitEvent(b->origin, b->join[i], 0);
   }
@@ -154,35 +132,43 @@ int batch_finish(sns_batch* b, const char* what) {
 // ---------------------------------------------------------------------------------------
 // Continuous-batching server.
 //
-// Memory: a solve's handle (fields, tables, stream) is not freed when the solve retires; it
-// joins an idle pool keyed by N and the next request of that N takes it over (its state
-// re-initialised in place), so a steady stream admits and retires without cudaMalloc or
-// cudaFree, which would synchronise the whole device.  The budget counts resident and idle
-// handles; an idle handle of another N is freed only when a request needs its room.
-// Time: a tick never waits for GPU work.  It launches a resident solve's next batch of
-// steps only when at most one earlier batch is still in flight (two batches queued per
-// solve keep the device busy between ticks), and retires a solve once the event after its
-// last step has completed, so requests are admitted and initialised while the others run.
+// Steps: every solve takes the reference's adaptive CFL step (ava_taylor_green_impl.hpp:
+// 1363-1378) at every step, computed on the device from the current state's vmax by the
+// handle's clock, and stops exactly at its horizon; one step is one graph replay, captured
+// once per handle.  After its horizon a replay leaves the state as it is.
+// Memory: a solve's handle (fields, tables, stream, graph) is not freed when the solve
+// retires; it joins an idle pool keyed by N and the next request of that N takes it over
+// (its state re-initialised in place), so a steady stream admits and retires without
+// cudaMalloc or cudaFree, which would synchronise the whole device.  The budget counts
+// resident and idle handles; an idle handle of another N is freed only when a request needs
+// its room.
+// Time: a tick never waits for GPU work.  It queues a resident solve's next batch of steps
+// only when at most one earlier batch is still in flight (two batches queued per solve keep
+// the device busy between ticks); each batch ends with a copy of the clock to pinned host
+// memory, from which the host learns the solve's time, and the solve retires once the
+// batch that reached the horizon has completed.
 struct sns_server {
   struct Pending {
     int64_t id;
     sns_request req;
   };
-  struct Slot {  // a handle with its own completion events, resident or idle
+  struct Slot {  // a handle with its step graph, events and clock copies, resident or idle
     sns_handle* h = nullptr;
+    cudaGraphExec_t step = nullptr;  // one adaptive step on the handle's clock
     cudaEvent_t ev[2] = {nullptr, nullptr};
+    double* snap = nullptr;          // pinned: the clock after batch 0 / 1 (kClockWords each)
     size_t bytes = 0;
     int n = 0;
   };
   struct Resident {
     Slot slot;
-    cudaGraphExec_t step = nullptr;  // one full step of size dt
     int64_t id = 0;
     sns_request req{};
-    double dt = 0.0, t = 0.0;
-    int steps = 0;
-    int head = 0;     // next event slot to record
-    int pending = 0;  // recorded batches not yet seen complete (0..2)
+    double t = 0.0, dt = 0.0;  // the clock as of the last completed batch
+    long long steps = 0;       // steps of the completed batches
+    long long launched = 0;    // steps queued so far
+    int head = 0;              // next event slot to record
+    int pending = 0;           // recorded batches not yet seen complete (0..2)
   };
   size_t budget = 0, used = 0, idle_bytes = 0;
   int precision = 0;
@@ -204,8 +190,10 @@ int server_fail(sns_server* s, int code, const std::string& msg) {
 }
 
 void free_slot(sns_server::Slot& sl) {
+  if (sl.step) cudaGraphExecDestroy(sl.step);
   for (cudaEvent_t& e : sl.ev)
     if (e) cudaEventDestroy(e);
+  if (sl.snap) cudaFreeHost(sl.snap);
   if (sl.h) sns_destroy(sl.h);
   sl = sns_server::Slot{};
 }
@@ -213,7 +201,6 @@ void free_slot(sns_server::Slot& sl) {
 // A retired solve's handle goes to the idle pool (no device memory is released).
 void retire(sns_server* s, size_t i) {
   sns_server::Resident& r = s->resident[i];
-  if (r.step) cudaGraphExecDestroy(r.step);
   s->used -= r.slot.bytes;
   s->idle_bytes += r.slot.bytes;
   s->idle.push_back(r.slot);
@@ -235,6 +222,43 @@ bool make_room(sns_server* s, size_t bytes) {
   return s->used + s->idle_bytes + bytes <= s->budget;
 }
 
+// A new handle of size n with its step graph, events and pinned clock copies.
+int make_slot(sns_server* s, const sns_request& q, size_t bytes, sns_server::Slot* out, std::string* err) {
+  sns_server::Slot sl;
+  int rc = sns_create(q.n, q.nu, s->precision, SNS_VISCOUS_EXPLICIT, q.seed, q.pert_amp, q.pert_kmax, &sl.h);
+  if (rc != SNS_OK) {
+    *err = sns_last_error(nullptr);
+    return rc;
+  }
+  sl.bytes = bytes;
+  sl.n = q.n;
+  cudaError_t e = cudaEventCreateWithFlags(&sl.ev[0], cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&sl.ev[1], cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaHostAlloc((void**)&sl.snap, 2 * sns::kClockWords * sizeof(double), cudaHostAllocDefault);
+  if (e != cudaSuccess) {
+    *err = cuda_msg("server slot", e);
+    free_slot(sl);
+    return SNS_ERR_CUDA;
+  }
+  // the graph: one adaptive step on the handle's clock (its step size is read on the device)
+  cudaStream_t st = sns::handle_stream(sl.h);
+  cudaGraph_t graph = nullptr;
+  e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    sns::enqueue_clock_step(sl.h);
+    e = cudaStreamEndCapture(st, &graph);
+  }
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&sl.step, graph, 0);
+  if (graph) cudaGraphDestroy(graph);
+  if (e != cudaSuccess) {
+    *err = cuda_msg("server step graph", e);
+    free_slot(sl);
+    return SNS_ERR_CUDA;
+  }
+  *out = sl;
+  return SNS_OK;
+}
+
 // Admit queued requests in arrival order while their device bytes fit the budget.
 int admit(sns_server* s) {
   while (!s->queue.empty()) {
@@ -250,46 +274,29 @@ int admit(sns_server* s) {
     sns_server::Resident r;
     r.id = p.id;
     r.req = p.req;
-    // an idle handle of this N: reuse it in place
     size_t k = 0;
     while (k < s->idle.size() && s->idle[k].n != p.req.n) ++k;
     int rc = SNS_OK;
+    std::string err;
     if (k < s->idle.size()) {
+      // an idle handle of this N: re-initialised in place, no allocation
       r.slot = s->idle[k];
       s->idle.erase(s->idle.begin() + (long)k);
       s->idle_bytes -= r.slot.bytes;
       rc = sns::reset_handle(r.slot.h, p.req.nu, p.req.seed, p.req.pert_amp, p.req.pert_kmax);
-      if (rc != SNS_OK) {
-        const std::string msg = sns_last_error(r.slot.h);
-        free_slot(r.slot);
-        s->queue.pop_front();
-        return server_fail(s, rc, "request " + std::to_string(p.id) + ": " + msg);
-      }
+      if (rc != SNS_OK) err = sns_last_error(r.slot.h);
     } else {
       if (!make_room(s, bytes)) return SNS_OK;  // waits until retirements free memory
-      rc = sns_create(p.req.n, p.req.nu, s->precision, SNS_VISCOUS_EXPLICIT, p.req.seed, p.req.pert_amp,
-                      p.req.pert_kmax, &r.slot.h);
+      rc = make_slot(s, p.req, bytes, &r.slot, &err);
       if (rc == SNS_ERR_NOMEM && !s->resident.empty()) return SNS_OK;  // the device itself is full: wait
-      if (rc != SNS_OK) {
-        s->queue.pop_front();
-        return server_fail(s, rc, "request " + std::to_string(p.id) + ": " + sns_last_error(nullptr));
-      }
-      ++s->allocations;
-      r.slot.bytes = bytes;
-      r.slot.n = p.req.n;
-      cudaError_t e = cudaEventCreateWithFlags(&r.slot.ev[0], cudaEventDisableTiming);
-      if (e == cudaSuccess) e = cudaEventCreateWithFlags(&r.slot.ev[1], cudaEventDisableTiming);
-      if (e != cudaSuccess) {
-        free_slot(r.slot);
-        s->queue.pop_front();
-        return server_fail(s, SNS_ERR_CUDA, cuda_msg("cudaEventCreate", e));
-      }
+      if (rc == SNS_OK) ++s->allocations;
     }
-    std::string err;
-    rc = choose_dt(r.slot.h, p.req.n, 0.0, p.req.cfl, p.req.dt_max, &r.dt, &err);
-    if (rc == SNS_OK) rc = capture_step(r.slot.h, r.dt, &r.step, &err);
+    if (rc == SNS_OK) {
+      rc = sns_set_clock(r.slot.h, 0.0, p.req.t_end, p.req.cfl, p.req.dt_max);
+      if (rc != SNS_OK) err = sns_last_error(r.slot.h);
+    }
     if (rc != SNS_OK) {
-      free_slot(r.slot);
+      if (r.slot.h) free_slot(r.slot);
       s->queue.pop_front();
       return server_fail(s, rc, "request " + std::to_string(p.id) + ": " + err);
     }
@@ -300,17 +307,24 @@ int admit(sns_server* s) {
   return SNS_OK;
 }
 
-// Has the older of the resident's in-flight batches completed?  Updates `pending`.
+// Take in the batches of the resident that have completed: `pending` drops and the host
+// copy of the clock advances to the latest completed batch's.
 int poll(sns_server* s, sns_server::Resident& r) {
   while (r.pending > 0) {
-    const cudaEvent_t oldest = r.slot.ev[(r.head + 2 - r.pending) & 1];
-    const cudaError_t e = cudaEventQuery(oldest);
+    const int idx = (r.head + 2 - r.pending) & 1;
+    const cudaError_t e = cudaEventQuery(r.slot.ev[idx]);
     if (e == cudaErrorNotReady) return SNS_OK;
     if (e != cudaSuccess) return server_fail(s, SNS_ERR_CUDA, cuda_msg("cudaEventQuery", e));
+    const double* c = r.slot.snap + idx * sns::kClockWords;
+    r.t = c[sns::kClockT];
+    if (c[sns::kClockDt] > 0.0) r.dt = c[sns::kClockDt];
+    r.steps = (long long)c[sns::kClockSteps];
     --r.pending;
   }
   return SNS_OK;
 }
+
+bool reached(const sns_server::Resident& r) { return !(r.t < r.req.t_end - 1.0e-14); }
 
 }  // namespace
 
@@ -329,6 +343,7 @@ int sns_batch_create(const sns_solve_spec* specs, int count, int autotune_trials
   cudaGetDevice(&b->device);
   b->h.assign(count, nullptr);
   b->dt.assign(count, 0.0);
+  b->adaptive.assign(count, 0);
   b->join.assign(count, nullptr);
   for (int i = 0; i < count; ++i) {
     const sns_solve_spec& sp = specs[i];
@@ -340,6 +355,12 @@ int sns_batch_create(const sns_solve_spec* specs, int count, int autotune_trials
     }
     std::string err;
     rc = choose_dt(b->h[i], sp.n, sp.dt, sp.cfl, sp.dt_max, &b->dt[i], &err);
+    if (rc == SNS_OK && !(sp.dt > 0.0)) {
+      // the reference's adaptive rule every step, on the device: no horizon
+      b->adaptive[i] = 1;
+      rc = sns_set_clock(b->h[i], 0.0, INFINITY, sp.cfl, sp.dt_max);
+      if (rc != SNS_OK) err = sns_last_error(b->h[i]);
+    }
     if (rc != SNS_OK) {
       sns::set_handleless_error(("sns_batch_create: solve " + std::to_string(i) + ": " + err).c_str());
       batch_release(b);
@@ -457,7 +478,6 @@ int sns_server_destroy(sns_server* s) {
   while (!s->resident.empty()) {
     sns_server::Resident& r = s->resident.back();
     cudaStreamSynchronize(sns::handle_stream(r.slot.h));
-    if (r.step) cudaGraphExecDestroy(r.step);
     free_slot(r.slot);
     s->resident.pop_back();
   }
@@ -484,51 +504,51 @@ int sns_server_step(sns_server* s, sns_result* done, int max_done, int* ndone, i
   cudaSetDevice(s->device);
   int rc = admit(s);
   if (rc != SNS_OK) return rc;
-  // Every resident solve with room in its two-batch window gets its next batch on its own
-  // stream: the largest by one step and smaller ones by proportionally more
+  // Every resident solve with room in its two-batch window gets its next batch of steps on
+  // its own stream: the largest by one step and smaller ones by proportionally more
   // (N_max^3 / N^3 steps, at most kMaxTickSteps), so a small solve is not held to the pace
-  // of the largest.  A full step replays the solve's graph; the last one (clipped to the
-  // horizon) is launched directly.
+  // of the largest; no more than the steps its horizon still needs at the last known step
+  // size (a step past the horizon is a no-op replay).
   constexpr double kMaxTickSteps = 64.0;
   double wmax = 0.0;
   for (const sns_server::Resident& r : s->resident) wmax = std::fmax(wmax, std::pow((double)r.req.n, 3.0));
   for (sns_server::Resident& r : s->resident) {
     rc = poll(s, r);
     if (rc != SNS_OK) return rc;
-    if (r.pending >= 2 || r.t >= r.req.t_end - 1.0e-12 * r.req.t_end) continue;
-    cudaStream_t st = sns::handle_stream(r.slot.h);
-    const int k = (int)std::fmin(kMaxTickSteps, std::fmax(1.0, std::floor(wmax / std::pow((double)r.req.n, 3.0))));
-    for (int j = 0; j < k && r.t < r.req.t_end - 1.0e-12 * r.req.t_end; ++j) {
-      const double left = r.req.t_end - r.t;
-      if (left >= r.dt - 1.0e-14 * r.req.t_end) {
-        const cudaError_t e = cudaGraphLaunch(r.step, st);
-        if (e != cudaSuccess) return server_fail(s, SNS_ERR_CUDA, cuda_msg("cudaGraphLaunch", e));
-        r.t += r.dt;
-      } else {
-        sns::enqueue_step(r.slot.h, left);
-        r.t = r.req.t_end;
-      }
-      ++r.steps;
+    if (r.pending >= 2 || reached(r)) continue;
+    long long k = (long long)std::fmin(kMaxTickSteps, std::fmax(1.0, std::floor(wmax / std::pow((double)r.req.n, 3.0))));
+    if (r.dt > 0.0) {
+      const long long need = (long long)std::ceil((r.req.t_end - r.t) / r.dt) + 1;
+      k = std::min(k, need - (r.launched - r.steps));
     }
-    const cudaError_t e = cudaEventRecord(r.slot.ev[r.head], st);
-    if (e != cudaSuccess) return server_fail(s, SNS_ERR_CUDA, cuda_msg("cudaEventRecord", e));
+    if (k <= 0) continue;
+    cudaStream_t st = sns::handle_stream(r.slot.h);
+    for (long long j = 0; j < k; ++j) {
+      const cudaError_t e = cudaGraphLaunch(r.slot.step, st);
+      if (e != cudaSuccess) return server_fail(s, SNS_ERR_CUDA, cuda_msg("cudaGraphLaunch", e));
+    }
+    r.launched += k;
+    double* snap = r.slot.snap + r.head * sns::kClockWords;
+    cudaError_t e = cudaMemcpyAsync(snap, sns::handle_clock(r.slot.h), sns::kClockWords * sizeof(double),
+                                    cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaEventRecord(r.slot.ev[r.head], st);
+    if (e != cudaSuccess) return server_fail(s, SNS_ERR_CUDA, cuda_msg("server batch", e));
     r.head ^= 1;
     ++r.pending;
   }
-  // retire the solves whose last step has completed
+  // retire the solves whose horizon a completed batch reached
   for (size_t i = s->resident.size(); i-- > 0;) {
     sns_server::Resident& r = s->resident[i];
-    if (r.t < r.req.t_end - 1.0e-12 * r.req.t_end) continue;
     rc = poll(s, r);
     if (rc != SNS_OK) return rc;
-    if (r.pending > 0) continue;
+    if (!reached(r) || r.pending > 0) continue;
     rc = sns::finish_handle(r.slot.h, "sns_server_step");  // the device error word
     if (rc != SNS_OK) return server_fail(s, rc, sns::handle_error(r.slot.h));
     sns_result res{};
     res.id = r.id;
     res.n = r.req.n;
-    res.steps = r.steps;
-    res.dt = r.dt;
+    res.steps = (int)r.steps;
+    res.dt = r.steps > 0 ? r.req.t_end / (double)r.steps : 0.0;
     rc = sns_diagnostics(r.slot.h, r.req.t_end, &res.final);
     if (rc != SNS_OK) return server_fail(s, rc, sns_last_error(r.slot.h));
     s->done.push_back(res);

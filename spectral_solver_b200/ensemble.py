@@ -3,9 +3,10 @@
 The ensemble configuration: solves with N drawn from {32, 48, 64, 96, 128}^3 (radix-2 and
 radix-3 plans) by ``numpy.random.default_rng(2026)``, Re log-uniform in [400, 3200], solve i
 perturbed with seed i (k^(-5/3), amplitude 1e-3, 1 <= |m| <= N/8), each with its own
-CFL-limited step (CFL 0.5), in the FP64 plain form and the FP32 precision form.  Every batch
-step is one CUDA graph launch with one branch per solve; launch shapes are autotuned once
-per (N, precision) and cached.
+CFL-limited step (CFL 0.5) recomputed on the device from its current vmax before every step,
+in the FP64 plain form and the FP32 precision form.  Every batch step is one CUDA graph
+launch with one branch per solve; launch shapes are autotuned once per (N, precision) and
+cached.
 
     python -m spectral_solver_b200.ensemble [--count 64] [--steps 500] [--warmup 3]
                                             [--precision both|fp64|fp32] [--autotune 2]

@@ -4,7 +4,8 @@ The sweep kernels carry each real part of u as hi + lo: hi = round-to-nearest FP
 FP64 update U, and the remainder U - hi as an int8 q, in units of ulp(hi) / 255, truncated
 toward zero after a nudge of 1e-6 away from it (comp_encode / comp_decode in
 spectral_solver_b200/csrc/sns_kernels.cu; ulp(hi) = 2^(E - 150) for the biased exponent E,
-taken as at least 1).  Three properties make the scheme work:
+taken as at least 1; multiplications by exact powers of two and by 255 or 1/255, no
+division).  Three properties make the scheme work:
 * decoding hi + q ulp / 255 in FP64 and encoding again gives the same pair (get_state ->
   set_state, checkpoint -> resume are exact);
 * round-to-nearest FP32 of the decoded value is hi (the stored FP32 value is the nearest
@@ -15,21 +16,24 @@ taken as at least 1).  Three properties make the scheme work:
 import numpy as np
 
 
+def exp_of(hi):
+    return np.maximum(((hi.view(np.uint32) >> 23) & 0xFF).astype(np.int64), 1)
+
+
 def ulp_of(hi):
-    e = ((hi.view(np.uint32) >> 23) & 0xFF).astype(np.int64)
-    return np.ldexp(1.0, np.maximum(e, 1) - 150)
+    return np.ldexp(1.0, exp_of(hi) - 150)
 
 
 def encode(U):
     hi = U.astype(np.float32)
-    r = (U - hi.astype(np.float64)) / ulp_of(hi) * 255.0
+    r = (U - hi.astype(np.float64)) * np.ldexp(1.0, 150 - exp_of(hi)) * 255.0
     q = np.trunc(r + np.copysign(1e-6, r)).astype(np.int64)
     assert np.all(np.abs(q) <= 127)
     return hi, q
 
 
 def decode(hi, q):
-    return hi.astype(np.float64) + (q * ulp_of(hi)) / 255.0
+    return hi.astype(np.float64) + q * ulp_of(hi) * (1.0 / 255.0)
 
 
 def cases():

@@ -42,10 +42,9 @@ def test_batch_matches_solves_alone(mod):
     for i, sp in enumerate(specs):
         with mod.Solver(sp["n"], 1.0 / sp["nu"], seed=sp["seed"], pert_amp=sp["pert_amp"], pert_kmax=sp["pert_kmax"],
                         precision=sp["precision"]) as s:
-            vmax = s.max_velocity()
-            dt = min(sp["dt_max"], sp["cfl"] * (2 * math.pi / sp["n"]) / vmax)
-            assert dt == dts[i]
-            s.step(dt, 3)
+            # every member takes the CFL step from its current vmax at every step
+            host_cfl_loop(s, sp["n"], float("inf"), 3, sp["cfl"], sp["dt_max"])
+            assert s.host_dts[0] == dts[i]
             ref = s.get_state()
         for a, r in zip(got[i], ref):
             assert np.array_equal(a, r), (i, sp["n"], sp["precision"])
@@ -61,6 +60,26 @@ def test_batch_timing_and_fixed_dt(mod):
     with mod.Solver(64, 1600.0) as s:
         s.step(5e-3, 4)
         assert s.diagnostics(0.02)["kinetic_energy"] == d["kinetic_energy"]
+
+
+def host_cfl_loop(s, n, t_end, max_steps, cfl=0.5, dt_max=0.5):
+    """The reference's adaptive loop (run_taylor_green, ava_taylor_green_impl.hpp:1363-1378)
+    on the host: vmax of the current state, dt = min(dt_max, cfl dx / vmax) clipped to the
+    horizon, one step.  Returns (steps, t) and the step sizes in s.host_dts."""
+    dx = 2.0 * math.pi / n
+    t, steps, dts = 0.0, 0, []
+    while t < t_end - 1e-14 and steps < max_steps:
+        vmax = s.max_velocity()
+        main_dt = dt_max
+        if vmax > 1e-14:
+            main_dt = min(main_dt, cfl * dx / vmax)
+        dt = min(main_dt, t_end - t)
+        s.step(dt)
+        t += dt
+        steps += 1
+        dts.append(dt)
+    s.host_dts = dts
+    return steps, t
 
 
 def run_server(mod, requests, budget, precision=FP32):
@@ -93,13 +112,10 @@ def test_server_result_same_alone_and_in_mix(mod):
     assert mixed[1]["steps"] == alone[0]["steps"] and mixed[1]["dt"] == alone[0]["dt"]
     for key in ("kinetic_energy", "dissipation", "enstrophy", "max_velocity"):
         assert mixed[1]["final"][key] == alone[0]["final"][key], key
-    # and the same as a handle stepped directly with the server's steps
+    # and the same as a handle stepped by the reference's adaptive loop on the host
     with mod.Solver(64, 1000.0, seed=7, pert_amp=1e-3, pert_kmax=8, precision=FP32) as s:
-        dt, t = alone[0]["dt"], 0.0
-        for _ in range(alone[0]["steps"]):
-            h = min(dt, a["t_end"] - t) if a["t_end"] - t < dt - 1e-14 * a["t_end"] else dt
-            s.step(h)
-            t += h
+        steps, t = host_cfl_loop(s, 64, a["t_end"], 10 ** 9)
+        assert steps == alone[0]["steps"]
         assert s.diagnostics(a["t_end"])["kinetic_energy"] == alone[0]["final"]["kinetic_energy"]
 
 
@@ -155,3 +171,47 @@ def test_server_reuses_retired_handles(mod):
         assert done[i]["steps"] == alone[0]["steps"]
         for key in ("kinetic_energy", "dissipation", "enstrophy", "max_velocity"):
             assert done[i]["final"][key] == alone[0]["final"][key], key
+
+
+@pytest.mark.parametrize("precision", [FP64, FP32])
+def test_device_clock_matches_host_adaptive_loop(mod, precision):
+    """sns_step_cfl takes the reference's adaptive step on the device: the same step sizes,
+    time and state, bit for bit, as the host loop over sns_max_velocity and sns_step; it
+    stops exactly at the horizon and later steps leave the state as it is."""
+    n, t_end = 48, 0.6
+    with mod.Solver(n, 900.0, seed=4, pert_amp=1e-2, pert_kmax=5, precision=precision) as host:
+        steps, t = host_cfl_loop(host, n, t_end, 10 ** 6)
+        ref = host.get_state()
+        dts = host.host_dts
+    with mod.Solver(n, 900.0, seed=4, pert_amp=1e-2, pert_kmax=5, precision=precision) as dev:
+        dev.set_clock(0.0, t_end, 0.5, 0.5)
+        for k in range(steps):
+            dev.step_cfl(1)
+            c = dev.clock()
+            assert c["dt"] == dts[k] and not c["stopped"], k
+        c = dev.clock()
+        assert c["t"] == t and c["steps"] == steps
+        dev.step_cfl(3)  # past the horizon: no-ops
+        c = dev.clock()
+        assert c["stopped"] and c["steps"] == steps
+        got = dev.get_state()
+    assert all(np.array_equal(a, b) for a, b in zip(got, ref))
+
+
+def test_batch_cfl_member_steps_like_host_loop(mod):
+    """A batch member with dt <= 0 takes the CFL step from its own vmax at every step, on
+    the device, inside the batch graph: after 15 batch steps its clock and state equal the
+    host adaptive loop's (no horizon)."""
+    specs = [dict(n=48, nu=1 / 700.0, dt=0.0, cfl=0.5, dt_max=0.5, seed=3, pert_amp=1e-2, pert_kmax=5),
+             dict(n=32, nu=1 / 500.0, dt=4e-3, seed=1, pert_amp=1e-3, pert_kmax=4)]
+    with mod.Batch(specs) as b:
+        b.step(15)
+        c = b.solver(0).clock()
+        got = b.solver(0).get_state()
+        first_dt = b.dt[0]
+    with mod.Solver(48, 700.0, seed=3, pert_amp=1e-2, pert_kmax=5) as s:
+        steps, t = host_cfl_loop(s, 48, float("inf"), 15)
+        ref = s.get_state()
+        assert s.host_dts[0] == first_dt
+    assert c["steps"] == 15 and c["t"] == t
+    assert all(np.array_equal(a, b) for a, b in zip(got, ref))
