@@ -6,7 +6,8 @@
   velocity) through the CLI, against the CPU oracle row by row;
 * the reference's published FP64 finals at t = 20 (Benchmark.md:644-649, 749-754,
   777-782) through the CLI with the benchmark's flags;
-* configuration 2's seeded field at 256^3: one RHS against the oracle (1e-12 relative L2);
+* configuration 2's seeded field at 256^3: one RHS against the oracle (1e-12 relative L2), and
+  its 100-step trajectory against the oracle's (a committed fixture), E and eps within 1e-10;
 * 100 steps of the seeded field at 128^3: kinetic energy and dissipation within 1e-10.
 """
 import csv
@@ -124,6 +125,43 @@ def test_seeded_trajectory_128_100_steps():
             for key in ("kinetic_energy", "dissipation"):
                 worst = max(worst, rel(d[key], dr[key]))
     assert worst <= 1e-10, worst
+
+
+def test_config2_trajectory_256_100_steps():
+    """Configuration 2 itself: the seeded 256^3 field, dt = 2.5e-3, 100 steps of the FP64
+    drop-in against the CPU oracle's trajectory (tests/golden/config2_256_trajectory.json,
+    made by tests/golden/make_config2_trajectory.py; the oracle takes ~35 min for it).
+    E, dissipation and enstrophy within 1e-10 relative every 10 steps; the final state's
+    per-component energy within 1e-10 relative and sampled modes within 1e-11 of the largest
+    mode amplitude."""
+    import json
+    from spectral_solver_b200 import Solver
+    with open(os.path.join(ROOT, "tests", "golden", "config2_256_trajectory.json")) as f:
+        gold = json.load(f)
+    n, dt = gold["n"], gold["dt"]
+    rows = {r["step"]: r for r in gold["rows"]}
+    with Solver(n, gold["reynolds"], seed=gold["seed"], pert_amp=gold["pert_amp"], pert_kmax=gold["pert_kmax"]) as s:
+        done = 0
+        for step in sorted(rows):
+            s.step(dt, step - done)
+            done = step
+            d, ref = s.diagnostics(step * dt), rows[step]
+            for key in ("kinetic_energy", "dissipation", "enstrophy"):
+                assert rel(d[key], ref[key]) <= 1e-10, (step, key, d[key], ref[key])
+            assert rel(d["max_velocity"], ref["max_velocity"]) <= 1e-9
+        assert done == gold["steps"] == 100
+        u = s.get_state()
+    half = [c[..., : n // 2 + 1] for c in u]
+    w = np.full(n // 2 + 1, 2.0)
+    w[0] = w[-1] = 1.0
+    for c in range(3):
+        assert rel(float(np.sum(w * np.abs(half[c]) ** 2)), gold["final_weighted_energy"][c]) <= 1e-10
+    amax = max(float(np.max(np.abs(c))) for c in half)
+    for smp in gold["final_samples"]:
+        mz, my, mx = smp["mode"]
+        for c in range(3):
+            want = complex(smp["re"][c], smp["im"][c])
+            assert abs(half[c][mz % n, my % n, mx] - want) <= 1e-11 * amax, (smp["mode"], c)
 
 
 def test_rhs_512_seeded():
