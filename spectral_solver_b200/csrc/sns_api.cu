@@ -826,6 +826,14 @@ int sns_set_viscosity(sns_handle* h, double nu) {
     return SNS_ERR_INVALID;
   }
   h->nu = nu;
+  // the device clock carries the viscosity for adaptive steps
+  if (cudaSetDevice(h->device) != cudaSuccess ||
+      cudaMemcpyAsync(h->clock + sns::kClockNu, &nu, sizeof(double), cudaMemcpyHostToDevice, h->stream) !=
+          cudaSuccess ||
+      cudaStreamSynchronize(h->stream) != cudaSuccess) {
+    h->err = std::string("sns_set_viscosity: ") + cudaGetErrorString(cudaGetLastError());
+    return SNS_ERR_CUDA;
+  }
   return SNS_OK;
 }
 
@@ -981,6 +989,7 @@ int sns_set_clock(sns_handle* h, double t, double t_end, double cfl, double dt_m
     c[sns::kClockCfl] = cfl;
     c[sns::kClockDtMax] = dt_max;
     c[sns::kClockDx] = 2.0 * kPi / static_cast<double>(h->n);
+    c[sns::kClockNu] = h->nu;
     ck(cudaMemcpyAsync(h->clock, c, sizeof c, cudaMemcpyHostToDevice, h->stream), "clock");
     sync(h, "sns_set_clock");
   });

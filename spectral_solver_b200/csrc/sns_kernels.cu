@@ -845,6 +845,7 @@ __device__ __forceinline__ SweepArgs resolve_step(SweepArgs a) {
   if (a.clock == nullptr) return a;
   const double dt = a.clock[kClockDt];
   a.frozen = a.clock[kClockStopped] != 0.0;
+  a.nu = a.clock[kClockNu];
   if (a.stage == 0) {
     a.ub = dt / 3.0;
     a.if_tau = dt / 3.0;

@@ -54,9 +54,10 @@ struct SweepArgs {
 };
 
 // Device clock of a solve stepped with an adaptive CFL step (doubles): the step size of the
-// current step, time, horizon, CFL number, step cap, grid spacing, steps taken, stopped flag.
-enum { kClockDt = 0, kClockT, kClockTEnd, kClockCfl, kClockDtMax, kClockDx, kClockSteps, kClockStopped,
-       kClockWords = 8 };
+// current step, time, horizon, CFL number, step cap, grid spacing, steps taken, stopped flag,
+// and the viscosity (so a step graph captured once serves every solve a pooled handle runs).
+enum { kClockDt = 0, kClockT, kClockTEnd, kClockCfl, kClockDtMax, kClockDx, kClockSteps, kClockStopped, kClockNu,
+       kClockWords = 9 };
 
 // Arguments of the TMA-fed streaming y/z pass.
 struct TmaArgs {
