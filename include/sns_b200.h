@@ -354,6 +354,15 @@ int sns_debug_set_error_word(sns_handle* h, int code);
  * current device and synchronises it.  Errors: sns_last_error(NULL). */
 int sns_debug_bounded_wait(unsigned polls, int* status);
 
+/* Debug-build hook: the index checks of libsns_b200_check.so (the same sources compiled with
+ * -DSNS_BOUNDS_CHECK; every shared-memory, tensor-memory and global index of the TMA-fed
+ * y/z passes, the two-stage x pass and the fused forward-z + sweep is checked against its
+ * buffer, recorded when outside it and replaced by 0).  *count receives the number of
+ * indices found outside their buffers so far in this process (-1 in the normal build, which
+ * has no checks), *line (may be NULL) the source line and *index (may be NULL) the value of
+ * the first. */
+int sns_debug_bounds(long long* count, int* line, long long* index);
+
 #ifdef __cplusplus
 }
 #endif

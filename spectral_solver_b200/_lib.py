@@ -11,7 +11,9 @@ import os
 import numpy as np
 
 _PKG = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_PKG, "libsns_b200.so")
+# SNS_B200_LIB=check loads the index-checked debug build (libsns_b200_check.so)
+LIB_PATH = os.path.join(_PKG, "libsns_b200_check.so" if os.environ.get("SNS_B200_LIB") == "check"
+                        else "libsns_b200.so")
 
 SNS_OK = 0
 SNS_ERR_INVALID = 1
@@ -82,6 +84,7 @@ SIGNATURES = {
     "sns_debug_fail_after": (C.c_int, [_H, C.c_int]),
     "sns_debug_set_error_word": (C.c_int, [_H, C.c_int]),
     "sns_debug_bounded_wait": (C.c_int, [C.c_uint, C.POINTER(C.c_int)]),
+    "sns_debug_bounds": (C.c_int, [C.POINTER(C.c_longlong), C.POINTER(C.c_int), C.POINTER(C.c_longlong)]),
     "sns_profile_passes": (C.c_int, [_H, C.c_double, C.c_int, _DP]),
     "sns_forward_r2c_noalloc": (C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
     "sns_batch_create": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_char_p, C.POINTER(C.c_void_p), _DP]),

@@ -1,6 +1,8 @@
 """In-tree build of the native parts (no JIT cache: the .so files travel with the tree).
 
 * ``libsns_b200.so``      CUDA kernels + C ABI (nvcc, sm_100a only)
+* ``libsns_b200_check.so`` the same with -DSNS_BOUNDS_CHECK: every index of the TMA /
+                          tensor-memory pass kernels checked against its buffer (tests only)
 * ``libspectral_b200.so`` C++ drop-in classes (B200Fft3D, SpectralNavierStokes,
                           TaylorGreenSolver, run_taylor_green) over the C ABI
 * ``bin/taylor_green_b200`` the reference's CLI (same flags and CSV)
@@ -29,6 +31,7 @@ NVFLAGS = ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr", "-Xcomp
            "-Xptxas", "-O3"]
 
 LIB = os.path.join(PKG, "libsns_b200.so")
+CHECK_LIB = os.path.join(PKG, "libsns_b200_check.so")
 HOSTLIB = os.path.join(PKG, "libspectral_b200.so")
 
 
@@ -56,22 +59,24 @@ def _run(cmd, verbose):
         print(r.stdout + r.stderr)
 
 
-def build_cuda(verbose=False, ptxas_verbose=False):
+def build_cuda(verbose=False, ptxas_verbose=False, check=False):
+    lib = CHECK_LIB if check else LIB
     cus = _sources(CSRC, (".cu",))
     deps = cus + _sources(CSRC, (".cuh", ".h")) + _sources(INC, (".h",))
-    if not _stale(LIB, deps) and not ptxas_verbose:
-        return LIB
-    objdir = os.path.join(PKG, "_build")
+    if not _stale(lib, deps) and not ptxas_verbose:
+        return lib
+    objdir = os.path.join(PKG, "_build", "check" if check else "")
     os.makedirs(objdir, exist_ok=True)
     objs = []
+    defs = ["-DSNS_BOUNDS_CHECK"] if check else []
     for cu in cus:
         obj = os.path.join(objdir, os.path.basename(cu) + ".o")
         extra = ["-Xptxas", "-v"] if ptxas_verbose else []
         if _stale(obj, [cu] + _sources(CSRC, (".cuh", ".h")) + _sources(INC, (".h",))) or ptxas_verbose:
-            _run([NVCC, *ARCH, *NVFLAGS, *extra, "-I", INC, "-c", cu, "-o", obj], verbose or ptxas_verbose)
+            _run([NVCC, *ARCH, *NVFLAGS, *defs, *extra, "-I", INC, "-c", cu, "-o", obj], verbose or ptxas_verbose)
         objs.append(obj)
-    _run([NVCC, *ARCH, "-shared", "-o", LIB, *objs, "-lcudart"], verbose)
-    return LIB
+    _run([NVCC, *ARCH, "-shared", "-o", lib, *objs, "-lcudart"], verbose)
+    return lib
 
 
 def build_host(verbose=False):
@@ -101,6 +106,7 @@ def build_host(verbose=False):
 def build(verbose=False):
     build_cuda(verbose)
     build_host(verbose)
+    build_cuda(verbose, check=True)
 
 
 if __name__ == "__main__":

@@ -57,3 +57,22 @@ extern "C" int sns_debug_bounded_wait(unsigned polls, int* status) {
   }
   return SNS_OK;
 }
+
+extern "C" int sns_debug_bounds(long long* count, int* line, long long* index) {
+  if (count == nullptr) {
+    sns::set_handleless_error("sns_debug_bounds: count must be non-null");
+    return SNS_ERR_INVALID;
+  }
+  long long r[3] = {0, 0, 0};
+  const int e = sns::bounds_record(r);
+  if (e != 0) {
+    char buf[200];
+    std::snprintf(buf, sizeof buf, "sns_debug_bounds: %s", cudaGetErrorString((cudaError_t)e));
+    sns::set_handleless_error(buf);
+    return SNS_ERR_CUDA;
+  }
+  *count = r[0];
+  if (line) *line = (int)r[1];
+  if (index) *index = r[2];
+  return SNS_OK;
+}

@@ -20,6 +20,8 @@
 
 #include <cuda_runtime.h>
 
+#include "sns_check.cuh"
+
 namespace sns {
 
 // Complex type traits and helpers (double2 / float2).
@@ -327,7 +329,7 @@ __device__ __forceinline__ void tstage(const Src& src, const Dst& dst, const C* 
       if constexpr (Ns > 1) {
         const int k = j % Ns;
 #pragma unroll
-        for (int r = 1; r < R; ++r) v[i][r] = cmul(v[i][r], stage_twiddle<DIR>(tw, r * k * kTwStep));
+        for (int r = 1; r < R; ++r) v[i][r] = cmul(v[i][r], stage_twiddle<DIR>(tw, SNS_IDX(r * k * kTwStep, L)));
       }
       dftR<R, DIR>(v[i]);
     }
@@ -349,12 +351,14 @@ __device__ __forceinline__ void tstage(const Src& src, const Dst& dst, const C* 
 template <int TW, class C>
 struct WLoad {
   const C* w;
-  __device__ __forceinline__ C operator()(int s, int e) const { return w[e * TW + s]; }
+  int n;  // elements of the work buffer (the index check of the debug build)
+  __device__ __forceinline__ C operator()(int s, int e) const { return w[SNS_IDX(e * TW + s, n)]; }
 };
 template <int TW, class C>
 struct WStore {
   C* w;
-  __device__ __forceinline__ void operator()(int s, int e, C v) const { w[e * TW + s] = v; }
+  int n;
+  __device__ __forceinline__ void operator()(int s, int e, C v) const { w[SNS_IDX(e * TW + s, n)] = v; }
 };
 
 template <int L, int DIR, int NT, int TW, int Ns, bool FIRST, class Src0, class DstG, class C, int R, int... Rest>
@@ -365,11 +369,11 @@ __device__ __forceinline__ void tfft_rec(const Src0& src0, C* W, const DstG& dst
   if constexpr (FIRST && LAST) {
     tstage<L, DIR, NT, TW, Ns, R, true, true>(src0, dstg, tw, tid);
   } else if constexpr (FIRST) {
-    tstage<L, DIR, NT, TW, Ns, R, true, false>(src0, WS{W}, tw, tid);
+    tstage<L, DIR, NT, TW, Ns, R, true, false>(src0, WS{W, L * TW}, tw, tid);
   } else if constexpr (LAST) {
-    tstage<L, DIR, NT, TW, Ns, R, false, true>(WL{W}, dstg, tw, tid);
+    tstage<L, DIR, NT, TW, Ns, R, false, true>(WL{W, L * TW}, dstg, tw, tid);
   } else {
-    tstage<L, DIR, NT, TW, Ns, R, false, false>(WL{W}, WS{W}, tw, tid);
+    tstage<L, DIR, NT, TW, Ns, R, false, false>(WL{W, L * TW}, WS{W, L * TW}, tw, tid);
   }
   if constexpr (!LAST) tfft_rec<L, DIR, NT, TW, Ns * R, false, Src0, DstG, C, Rest...>(src0, W, dstg, tw, tid);
 }
@@ -441,10 +445,10 @@ __device__ __forceinline__ void tfft_sink_rec(const Src0& src0, C* W, const C* t
   using WS = WStore<TW, C>;
   if constexpr (sizeof...(Rest) == 0) {
     if constexpr (FIRST) tstage_sink<L, DIR, NT, TW, Ns, R>(src0, tw, tid, sink);
-    else tstage_sink<L, DIR, NT, TW, Ns, R>(WL{W}, tw, tid, sink);
+    else tstage_sink<L, DIR, NT, TW, Ns, R>(WL{W, L * TW}, tw, tid, sink);
   } else {
-    if constexpr (FIRST) tstage<L, DIR, NT, TW, Ns, R, true, false>(src0, WS{W}, tw, tid);
-    else tstage<L, DIR, NT, TW, Ns, R, false, false>(WL{W}, WS{W}, tw, tid);
+    if constexpr (FIRST) tstage<L, DIR, NT, TW, Ns, R, true, false>(src0, WS{W, L * TW}, tw, tid);
+    else tstage<L, DIR, NT, TW, Ns, R, false, false>(WL{W, L * TW}, WS{W, L * TW}, tw, tid);
     tfft_sink_rec<L, DIR, NT, TW, Ns * R, false, Src0, Sink, C, Rest...>(src0, W, tw, tid, sink);
   }
 }

@@ -251,21 +251,21 @@ k_yz_tma(const __grid_constant__ CUtensorMap map, TmaArgs a, const C* __restrict
     if constexpr (VARIANT == 0) {
       C* outf = static_cast<C*>(a.out) + (long long)(a.f_out0 + fi) * g.field;
       auto src = [&](int s, int e) {
-        const C v = IN[e * TW + s];
+        const C v = IN[SNS_IDX(e * TW + s, TW * N)];
         return sc == RT(1) ? v : cscale(v, sc);
       };
       auto dst = [&](int s, int e, C v) {
         const long long at = AXIS == 1 ? ((long long)c * N + e) * g.pitch : ((long long)e * N + c) * g.pitch;
-        outf[at + mx0 + s] = v;
+        outf[SNS_IDX(at + mx0 + s, g.field)] = v;
       };
       tile_fft<N, DIR, NT, TW>(src, W, dst, s_tw, tid);
     } else {
       static_assert(AXIS == 2, "phase variant is the inverse z pass");
       C* out_u = static_cast<C*>(a.out) + (long long)(a.f_out0 + 2 * fi) * g.field;
       C* out_v = out_u + g.field;
-      auto dst_u = [&](int s, int e, C v) { out_u[((long long)e * N + c) * g.pitch + mx0 + s] = v; };
-      auto dst_v = [&](int s, int e, C v) { out_v[((long long)e * N + c) * g.pitch + mx0 + s] = v; };
-      auto src_u = [&](int s, int e) { return cscale(IN[e * TW + s], sc); };
+      auto dst_u = [&](int s, int e, C v) { out_u[SNS_IDX(((long long)e * N + c) * g.pitch + mx0 + s, g.field)] = v; };
+      auto dst_v = [&](int s, int e, C v) { out_v[SNS_IDX(((long long)e * N + c) * g.pitch + mx0 + s, g.field)] = v; };
+      auto src_u = [&](int s, int e) { return cscale(IN[SNS_IDX(e * TW + s, TW * N)], sc); };
       tile_fft<N, DIR, NT, TW>(src_u, W, dst_u, s_tw, tid);
       __syncthreads();
       const int smy = signed_mode(c, N);
@@ -276,8 +276,8 @@ k_yz_tma(const __grid_constant__ CUtensorMap map, TmaArgs a, const C* __restrict
         const int mx = mx0 + s;
         const bool anti = mx > 0 && mx < N / 2 && ((c == N / 2) != (e == N / 2));
         if (mx > N / 2 || anti) return czero<C>();
-        const C v = cscale(IN[e * TW + s], sc);
-        return cmul(v, __ldg(&phase[mx + smy + signed_mode(e, N) + 3 * N / 2]));
+        const C v = cscale(IN[SNS_IDX(e * TW + s, TW * N)], sc);
+        return cmul(v, __ldg(&phase[SNS_IDX(mx + smy + signed_mode(e, N) + 3 * N / 2, 3 * N + 1)]));
       };
       tile_fft<N, DIR, NT, TW>(src_v, W, dst_v, s_tw, tid);
     }
@@ -509,7 +509,7 @@ k_xpass2(C* __restrict__ work, const C* __restrict__ unyq, const C* __restrict__
       const long long row = it * ROWS + r;
 #pragma unroll
       for (int f = 0; f < 6; ++f)
-        bulk_load(stg + (b * ROWS + r) * STG + f * RS, work + (long long)f * g.field + row * g.pitch,
+        bulk_load(stg + (b * ROWS + r) * STG + f * RS, work + (long long)f * g.field + SNS_IDX(row, (long long)N * N) * g.pitch,
                   X::kRowBytes, &bars[b]);
     }
   };
@@ -564,7 +564,7 @@ k_xpass2(C* __restrict__ work, const C* __restrict__ unyq, const C* __restrict__
         if (x == 0) {
           z = cmk(Ur[0].x, Vr[0].x);
         } else if (x < NH) {
-          const C U = Ur[x], V = Vr[x];
+          const C U = Ur[SNS_IDX(x, RS)], V = Vr[SNS_IDX(x, RS)];
           z = cmk(U.x - V.y, U.y + V.x);
         } else if (x == NH) {
           C U, V;
@@ -577,7 +577,7 @@ k_xpass2(C* __restrict__ work, const C* __restrict__ unyq, const C* __restrict__
           }
           z = cmk(U.x, V.x);
         } else {
-          const C U = Ur[N - x], V = Vr[N - x];
+          const C U = Ur[SNS_IDX(N - x, RS)], V = Vr[SNS_IDX(N - x, RS)];
           z = cmk(U.x + V.y, V.x - U.y);
         }
         v[q] = z;
@@ -585,7 +585,7 @@ k_xpass2(C* __restrict__ work, const C* __restrict__ unyq, const C* __restrict__
       dft16<+1>(v);
       C* Wc = W + (r * 6 + c) * SP;
 #pragma unroll
-      for (int q = 0; q < 16; ++q) Wc[pp16(16 * t + q)] = v[q];
+      for (int q = 0; q < 16; ++q) Wc[SNS_IDX(pp16(16 * t + q), SP)] = v[q];
     }
     __syncwarp();
 
@@ -598,7 +598,7 @@ k_xpass2(C* __restrict__ work, const C* __restrict__ unyq, const C* __restrict__
 #pragma unroll
         for (int i = 0; i < 16; ++i) {
           const int rr = 2 * i + h;
-          v[i] = cmulc(Wc[pp16(j + 16 * rr)], stage_b_tw(i, j, h));  // inverse twiddle = conj
+          v[i] = cmulc(Wc[SNS_IDX(pp16(j + 16 * rr), SP)], stage_b_tw(i, j, h));  // inverse twiddle = conj
         }
         dft16<+1>(v);
         if (h) {
@@ -610,7 +610,7 @@ k_xpass2(C* __restrict__ work, const C* __restrict__ unyq, const C* __restrict__
         for (int q = 0; q < 16; ++q) {
           const C o = shfl2_xor(v[q], 16);
           const C z = h ? csub(o, v[q]) : cadd(v[q], o);
-          Zc[pp16(j + 16 * (q + 16 * h))] = z;
+          Zc[SNS_IDX(pp16(j + 16 * (q + 16 * h)), SP)] = z;
         }
       }
     } else {
@@ -619,11 +619,12 @@ k_xpass2(C* __restrict__ work, const C* __restrict__ unyq, const C* __restrict__
         const C* Wc = W + (r * 6 + c) * SP;
         C v[16];
 #pragma unroll
-        for (int q = 0; q < 16; ++q) v[q] = q == 0 ? Wc[pp16(j)] : cmulc(Wc[pp16(j + 16 * q)], tw2[q * 16 + j]);
+        for (int q = 0; q < 16; ++q)
+          v[q] = q == 0 ? Wc[pp16(j)] : cmulc(Wc[SNS_IDX(pp16(j + 16 * q), SP)], tw2[SNS_IDX(q * 16 + j, N)]);
         dft16<+1>(v);
         C* Zc = W + (r * 6 + 3 + c) * SP;
 #pragma unroll
-        for (int q = 0; q < 16; ++q) Zc[pp16(j + 16 * q)] = v[q];
+        for (int q = 0; q < 16; ++q) Zc[SNS_IDX(pp16(j + 16 * q), SP)] = v[q];
       }
     }
     __syncthreads();
@@ -646,7 +647,7 @@ k_xpass2(C* __restrict__ work, const C* __restrict__ unyq, const C* __restrict__
         C v[16];
 #pragma unroll
         for (int q = 0; q < 16; ++q) {
-          const int x = pp16(t + M * q);
+          const int x = SNS_IDX(pp16(t + M * q), SP);
           const C za = Za[x];
           const C zb = ca == cb ? za : Zb[x];  // squares 00, 11, 22: one load
           v[q] = cmk(za.x * zb.x, za.y * zb.y);
@@ -654,7 +655,7 @@ k_xpass2(C* __restrict__ work, const C* __restrict__ unyq, const C* __restrict__
         dft16<-1>(v);
         C* Wp = prod(r, ab);
 #pragma unroll
-        for (int q = 0; q < 16; ++q) Wp[pp16(16 * t + q)] = v[q];
+        for (int q = 0; q < 16; ++q) Wp[SNS_IDX(pp16(16 * t + q), SP)] = v[q];
       }
       __syncwarp();
 
@@ -667,7 +668,7 @@ k_xpass2(C* __restrict__ work, const C* __restrict__ unyq, const C* __restrict__
 #pragma unroll
         for (int i = 0; i < 16; ++i) {
           const int rr = 2 * i + h;
-          v[i] = cmul(Wp[pp16(j + 16 * rr)], stage_b_tw(i, j, h));
+          v[i] = cmul(Wp[SNS_IDX(pp16(j + 16 * rr), SP)], stage_b_tw(i, j, h));
         }
         dft16<-1>(v);
         if (h) {
@@ -692,8 +693,8 @@ k_xpass2(C* __restrict__ work, const C* __restrict__ unyq, const C* __restrict__
           if (kk <= NH) {
             C A, B;
             unpack_pair(v[i], zm, &A, &B);
-            o0[kk] = A;
-            o1[kk] = B;
+            o0[SNS_IDX(kk, g.pitch)] = A;
+            o1[SNS_IDX(kk, g.pitch)] = B;
             if (kk == NH) {
               nyq_p0 += A.x;
               nyq_ps += B.x;
@@ -705,7 +706,8 @@ k_xpass2(C* __restrict__ work, const C* __restrict__ unyq, const C* __restrict__
         const C* Wp = prod(r, ab);
         C v[16];
 #pragma unroll
-        for (int q = 0; q < 16; ++q) v[q] = q == 0 ? Wp[pp16(j)] : cmul(Wp[pp16(j + 16 * q)], tw2[q * 16 + j]);
+        for (int q = 0; q < 16; ++q)
+          v[q] = q == 0 ? Wp[pp16(j)] : cmul(Wp[SNS_IDX(pp16(j + 16 * q), SP)], tw2[SNS_IDX(q * 16 + j, N)]);
         dft16<-1>(v);
         const int lane = tid & 31;
         const int partner = (lane & 16) + ((16 - j) & 15);
@@ -720,8 +722,8 @@ k_xpass2(C* __restrict__ work, const C* __restrict__ unyq, const C* __restrict__
           if (kk <= NH) {
             C A, B;
             unpack_pair(v[q], zm, &A, &B);
-            o0[kk] = A;
-            o1[kk] = B;
+            o0[SNS_IDX(kk, g.pitch)] = A;
+            o1[SNS_IDX(kk, g.pitch)] = B;
             if (kk == NH) {
               nyq_p0 += A.x;
               nyq_ps += B.x;
@@ -1355,7 +1357,7 @@ k_p5(const __grid_constant__ CUtensorMap map, C* __restrict__ u, C* __restrict__
   // only the listed ones
   const long long ntiles = live ? (long long)nlive : (long long)ncb * N;
   auto tile_of = [&](long long t, int& cb, int& my) {
-    const int idx = live ? __ldg(&live[t]) : (int)t;
+    const int idx = live ? __ldg(&live[SNS_IDX(t, nlive)]) : (int)t;
     my = idx / ncb;
     cb = idx - my * ncb;
   };
@@ -1405,6 +1407,9 @@ k_p5(const __grid_constant__ CUtensorMap map, C* __restrict__ u, C* __restrict__
       constexpr int R = RO::R, NS = RO::NS;
       const int bb = tid + i * NT, s_ = bb % TW, j = bb / TW;
       const uint32_t col = (uint32_t)(WPC * R * i);
+      // tensor-memory columns of this thread's blocks stay inside the allocation
+      (void)SNS_IDX((warp >> 2) * 4 * CW + 4 * CW - 1, (long long)COLS);
+      (void)SNS_IDX(col + WPC * R - 1, (long long)CW);
       if ((f & 1) == 0) {
         tmem_st<R>(tq + col, v);  // park P0 of this pair
         return;
@@ -1418,7 +1423,8 @@ k_p5(const __grid_constant__ CUtensorMap map, C* __restrict__ u, C* __restrict__
         for (int r = 0; r < R; ++r) {
           izs[r] = signed_mode((j / NS) * NS * R + (j % NS) + r * NS, N);
           const bool keep = 4LL * (ix * ix + iy * iy + izs[r] * izs[r]) <= (long long)N * N;
-          v[r] = pair_value(p0[r], v[r], __ldg(&phase[ix + iy + izs[r] + 3 * N / 2]), keep, a.dealias);
+          v[r] = pair_value(p0[r], v[r], __ldg(&phase[SNS_IDX(ix + iy + izs[r] + 3 * N / 2, 3 * N + 1)]), keep,
+                            a.dealias);
         }
       }
       // r_a += -i k_b value; r_b += -i k_a value (a != b); the first touch starts the sum
@@ -1439,7 +1445,8 @@ k_p5(const __grid_constant__ CUtensorMap map, C* __restrict__ u, C* __restrict__
         tmem_st<R>(ta, r);
       }
     };
-    tile_fft_sink<N, -1, NT, TW>([&](int s_, int e_) { return IN[e_ * TW + s_]; }, W, s_tw, tid, sink);
+    tile_fft_sink<N, -1, NT, TW>([&](int s_, int e_) { return IN[SNS_IDX(e_ * TW + s_, TW * N)]; }, W, s_tw, tid,
+                                 sink);
     tmem_wait_st();
     __syncthreads();  // IN[b] and W are free again
     if (tid == 0 && ul + 2 < nunits) issue(ul + 2, b);
@@ -1454,7 +1461,7 @@ k_p5(const __grid_constant__ CUtensorMap map, C* __restrict__ u, C* __restrict__
       C uu_n[3], gg_n[3];
       CompWord lo_n[3] = {0, 0, 0};
       auto load_mode = [&](int q, C* uu, C* gg, CompWord* lo) {
-        const long long idx = ((long long)mode_e(q) * N + my) * g.pitch + mx0 + mode_s(q);
+        const long long idx = SNS_IDX(((long long)mode_e(q) * N + my) * g.pitch + mx0 + mode_s(q), g.field);
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
           uu[c] = u[(long long)c * g.field + idx];
@@ -1482,10 +1489,10 @@ k_p5(const __grid_constant__ CUtensorMap map, C* __restrict__ u, C* __restrict__
         const int ez = mode_e(q);
         const int iz = signed_mode(ez, N);
         const long long row = (long long)ez * N + my;
-        const long long idx = row * g.pitch + ix;
+        const long long idx = SNS_IDX(row * g.pitch + ix, g.field);
         finish_mode(r3, ix, iy, iz, N, uu, gg, load_g, rr, a, lo);
         const bool nyq_zero = ix == 0 && row != 0;  // plane mx = N/2 is zero off (N/2,0,0)
-        const long long inq = row * g.pitch + NH;
+        const long long inq = SNS_IDX(row * g.pitch + NH, g.field);
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
           if (a.mode != 0) {
@@ -2117,6 +2124,24 @@ __global__ void k_clock_step(const double* __restrict__ vmax2, double* __restric
   c[kClockDt] = dt;
   c[kClockT] = t + dt;
   c[kClockSteps] += 1.0;
+}
+
+// The index-check record of the debug build: {count, first line, first index}; count -1 in
+// the normal build, which has no checks.
+int bounds_record(long long* out3) {
+#ifdef SNS_BOUNDS_CHECK
+  BoundsRecord r{};
+  const cudaError_t e = cudaMemcpyFromSymbol(&r, g_bounds, sizeof r);
+  if (e != cudaSuccess) return (int)e;
+  out3[0] = (long long)r.count;
+  out3[1] = r.line;
+  out3[2] = r.index;
+#else
+  out3[0] = -1;
+  out3[1] = 0;
+  out3[2] = 0;
+#endif
+  return 0;
 }
 
 void launch_clock_step(const double* vmax2, double* clock, cudaStream_t st) {
