@@ -363,6 +363,15 @@ int sns_debug_bounded_wait(unsigned polls, int* status);
  * the first. */
 int sns_debug_bounds(long long* count, int* line, long long* index);
 
+/* Measurement hook: `count` (a positive multiple of 128) 16-point complex DFTs (sign -1,
+ * unnormalised; FP32 re/im interleaved, 32 floats per sequence, device buffers 16-byte
+ * aligned) from dev_in to dev_out on `stream`, either on the register butterflies the pass
+ * kernels use (use_tensor_cores = 0) or as tcgen05.mma kind::tf32 tiles of 128 sequences
+ * with the 3xTF32 split (1).  *elapsed_ms (may be NULL) receives the kernel's CUDA-event
+ * time.  Synchronises the stream.  Errors: sns_last_error(NULL). */
+int sns_dft16_batch(const float* dev_in, float* dev_out, long long count, int use_tensor_cores, void* stream,
+                    double* elapsed_ms);
+
 #ifdef __cplusplus
 }
 #endif

@@ -85,6 +85,7 @@ SIGNATURES = {
     "sns_debug_set_error_word": (C.c_int, [_H, C.c_int]),
     "sns_debug_bounded_wait": (C.c_int, [C.c_uint, C.POINTER(C.c_int)]),
     "sns_debug_bounds": (C.c_int, [C.POINTER(C.c_longlong), C.POINTER(C.c_int), C.POINTER(C.c_longlong)]),
+    "sns_dft16_batch": (C.c_int, [C.c_void_p, C.c_void_p, C.c_longlong, C.c_int, C.c_void_p, _DP]),
     "sns_profile_passes": (C.c_int, [_H, C.c_double, C.c_int, _DP]),
     "sns_forward_r2c_noalloc": (C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
     "sns_batch_create": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_char_p, C.POINTER(C.c_void_p), _DP]),

@@ -85,6 +85,15 @@ def test_batch_and_server_reject_bad_arguments(lib):
     assert len(lib.sns_last_error(None)) > 0
 
 
+def test_dft16_batch_rejects_bad_arguments(lib):
+    buf = C.c_void_p(1 << 20)  # never dereferenced: the arguments are refused first
+    assert lib.sns_dft16_batch(None, buf, 128, 1, None, None) == 1
+    assert lib.sns_dft16_batch(buf, buf, 100, 1, None, None) == 1  # not a multiple of 128
+    assert lib.sns_dft16_batch(buf, buf, 128, 2, None, None) == 1  # unknown method
+    assert lib.sns_dft16_batch(C.c_void_p((1 << 20) + 4), buf, 128, 0, None, None) == 1  # unaligned
+    assert b"sns_dft16_batch" in lib.sns_last_error(None)
+
+
 @pytest.mark.skipif(has_gpu(), reason="checks the no-device path")
 def test_no_device_is_reported(lib):
     h = C.c_void_p()
