@@ -68,6 +68,33 @@ template <class C>
 __host__ __device__ __forceinline__ C cmul(C a, C b) {
   return cmk(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
+// FP32 complex add and subtract as one packed instruction on the register pair (sm_100's
+// add.f32x2 / sub.f32x2: two IEEE single-precision operations, round to nearest, the same
+// results as two scalar ones).  Opt-in: the two-stage x pass is bound by instruction issue
+// and most of its arithmetic is butterfly additions, so it takes them; in the y/z passes and
+// the fused sweep they cost 2-3 % (additions there often absorb a product into an FFMA,
+// which a packed add prevents), so those keep the scalar forms.
+__device__ __forceinline__ unsigned long long f2_pack(float2 a) {
+  unsigned long long r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a.x), "f"(a.y));
+  return r;
+}
+__device__ __forceinline__ float2 f2_unpack(unsigned long long r) {
+  float2 a;
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(a.x), "=f"(a.y) : "l"(r));
+  return a;
+}
+__device__ __forceinline__ float2 padd(float2 a, float2 b) {
+  unsigned long long d;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(f2_pack(a)), "l"(f2_pack(b)));
+  return f2_unpack(d);
+}
+__device__ __forceinline__ float2 psub(float2 a, float2 b) {
+  unsigned long long d;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(f2_pack(a)), "l"(f2_pack(b)));
+  return f2_unpack(d);
+}
+
 // a * conj(b)
 template <class C>
 __host__ __device__ __forceinline__ C cmulc(C a, C b) {
@@ -123,6 +150,22 @@ __host__ __device__ __forceinline__ void dft4(C* v) {
   v[1] = cadd(s1, s3);
   v[3] = csub(s1, s3);
 }
+// FP32 with packed additions: the six plain additions packed; the two that take +-i (b - d)
+// stay scalar, so the swapped pair is never formed.  Same results as dft4<DIR, float2>.
+template <int DIR>
+__device__ __forceinline__ void dft4p(float2* v) {
+  const float2 a = v[0], b = v[1], c = v[2], d = v[3];
+  const float2 s0 = padd(a, c), s1 = psub(a, c), s2 = padd(b, d), t = psub(b, d);
+  v[0] = padd(s0, s2);
+  v[2] = psub(s0, s2);
+  if constexpr (DIR < 0) {  // s3 = -i t
+    v[1] = make_float2(s1.x + t.y, s1.y - t.x);
+    v[3] = make_float2(s1.x - t.y, s1.y + t.x);
+  } else {  // s3 = +i t
+    v[1] = make_float2(s1.x - t.y, s1.y + t.x);
+    v[3] = make_float2(s1.x + t.y, s1.y - t.x);
+  }
+}
 
 template <int DIR, class C>
 __host__ __device__ __forceinline__ void dft8(C* v) {
@@ -151,7 +194,8 @@ __host__ __device__ __forceinline__ void dft8(C* v) {
 
 // 16-point DFT in registers, natural order in and out: 4 x 4 Cooley-Tukey
 // (inner 4-point DFTs over stride-4 inputs, twiddles W16^(n2*k1), outer 4-point DFTs).
-template <int DIR, class C>
+// PK: the 4-point DFTs with packed FP32 additions (C = float2, device code only).
+template <int DIR, class C, bool PK = false>
 __host__ __device__ __forceinline__ void dft16(C* v) {
   using RT = real_of<C>;
   constexpr RT c1 = RT(0.92387953251128675612818318939678829);  // cos(pi/8)
@@ -161,7 +205,8 @@ __host__ __device__ __forceinline__ void dft16(C* v) {
 #pragma unroll
   for (int n2 = 0; n2 < 4; ++n2) {
     C t[4] = {v[n2], v[n2 + 4], v[n2 + 8], v[n2 + 12]};
-    dft4<DIR>(t);
+    if constexpr (PK) dft4p<DIR>(t);
+    else dft4<DIR>(t);
 #pragma unroll
     for (int k1 = 0; k1 < 4; ++k1) a[n2][k1] = t[k1];
   }
@@ -181,7 +226,8 @@ __host__ __device__ __forceinline__ void dft16(C* v) {
 #pragma unroll
   for (int k1 = 0; k1 < 4; ++k1) {
     C t[4] = {a[0][k1], a[1][k1], a[2][k1], a[3][k1]};
-    dft4<DIR>(t);
+    if constexpr (PK) dft4p<DIR>(t);
+    else dft4<DIR>(t);
 #pragma unroll
     for (int k2 = 0; k2 < 4; ++k2) v[k1 + 4 * k2] = t[k2];
   }

@@ -22,6 +22,7 @@
 #include "sns_tma.cuh"
 
 #include <algorithm>
+#include <type_traits>
 #include <cstdio>
 
 namespace sns {
@@ -751,6 +752,258 @@ k_xpass2(C* __restrict__ work, const C* __restrict__ unyq, const C* __restrict__
     }
     __syncthreads();
     if (tid < 12) nyq_part[tid * gridDim.x + blockIdx.x] = s_nyq[0][tid] + s_nyq[1][tid];
+  }
+}
+
+// ---------------------------------------------------------------------------------------
+// x pass of the FP32 form at N = 256 and 512: one warp owns R = 512 / N rows at a time and
+// runs every stage of them alone, so the CTA (eight warps, one CTA per SM) never
+// synchronises inside the loop.  The same operation as k_xpass2 (reference: the nonlinear
+// term of spectral_solver.cpp:93-158, 169-215 on the r2c layout), reorganised so the three
+// inverse transforms meet the products in registers:
+//   inverse stage A  lane t (of M = N/16) per row: 16-point DFTs over x = t + M q, packing
+//                    z_c = U_c + i V_c fused into the staged-row loads; out to Wc[c][t][k].
+//                    The staging buffer is then free: the next row group's bulk copy is
+//                    issued into it and lands while the rest of this group is transformed.
+//   inverse stage B  lane (j, h): the M-point DFT over t at fixed k = j (four-step twiddle
+//                    W_N^(j t) before; at N = 512 two half-warps and one shuffle), leaving
+//                    z_c(x) for x = j + 16 n, n of the lane, of all three components in
+//                    registers
+//   products + forward stage A  per product u_a u_b (both grids: real and imaginary part)
+//                    the M-point DFT over n at fixed j (at N = 512 split in frequency: one
+//                    shuffle, then a 16-point DFT), times W_N^(j k1); out to P[ab][j][k1]
+//   forward stage B  lane k1: the 16-point DFT over j, outputs k1 + M k2; r2c unpack of the
+//                    two grids through the partner lane (N - k), 128-byte stores to HBM
+// The products run in two halves of three (00 01 02, then 11 12 22), each through Wc and its
+// forward stage B, so a warp holds one staged row group and one transposition buffer.  Every
+// transposition goes through shared memory once, XOR-swizzled (no bank conflicts); the
+// products never do.  The kernel is bound by instruction issue, so its complex additions run
+// as packed FP32 pairs (padd / psub, dft16<.., true>): the same results in fewer instructions.
+template <int N>
+struct XW {
+  using C = float2;
+  static constexpr int M = N / 16;      // inverse stage-A lanes per row, forward stage-B lanes
+  static constexpr int R = 512 / N;     // rows per warp (32 lanes = R * M)
+  static constexpr int NH = N / 2;
+  static constexpr int WARPS = 8;
+  static constexpr int RS = (int)(((NH + 1) * sizeof(C) + 15) / 16 * 16 / sizeof(C));  // staged row
+  static constexpr int STG = R * 6 * RS;  // the staging buffer: [R][6 fields][RS]
+  static constexpr int WC = R * 3 * N;    // transposition buffer [R][3][N]
+  static constexpr int PER_WARP = STG + WC;
+  static constexpr uint32_t kRowBytes = RS * sizeof(C);
+  static constexpr size_t smem =
+      (size_t)WARPS * PER_WARP * sizeof(C) + 128 + WARPS * (sizeof(uint64_t) + R * 12 * sizeof(double));
+  static_assert(R * M == 32, "a warp covers its rows' lanes");
+};
+
+template <int N>
+__global__ void __launch_bounds__(32 * XW<N>::WARPS, 1)
+k_xpass_w(float2* __restrict__ work, const float2* __restrict__ unyq, const float2* __restrict__ phase, double scale,
+          int nyq_scalar, double* __restrict__ nyq_part, const float2* __restrict__ tw2_g, Geom g, int* err) {
+  using X = XW<N>;
+  using C = float2;
+  constexpr int M = X::M, R = X::R, NH = X::NH, RS = X::RS;
+  constexpr unsigned kFull = 0xffffffffu;
+  extern __shared__ unsigned char smraw[];
+  const uint32_t pad = (128u - (smem_u32(smraw) & 127u)) & 127u;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  C* const all = reinterpret_cast<C*>(smraw + pad);
+  C* const stg = all + warp * X::PER_WARP;  // [R][6][RS]
+  C* const Wc = stg + X::STG;               // [R][3][N], element (t, k) at 16 t + (k ^ (t & 15))
+  uint64_t* const bar = reinterpret_cast<uint64_t*>(all + X::WARPS * X::PER_WARP) + warp;
+  double* const s_nyq =
+      reinterpret_cast<double*>(reinterpret_cast<uint64_t*>(all + X::WARPS * X::PER_WARP) + X::WARPS);
+  double* const my_nyq = s_nyq + warp * R * 12;  // [WARPS][R][12]
+  if (lane < R * 12) my_nyq[lane] = 0.0;
+  if (lane == 0) {
+    mbar_init(bar, 1);
+    fence_mbar_init();
+  }
+  __syncwarp();
+  const long long niter = (long long)N * N / R;
+  const long long gw = (long long)blockIdx.x * X::WARPS + warp, nw = (long long)gridDim.x * X::WARPS;
+  auto issue = [&](long long it) {
+    mbar_arrive_expect_tx(bar, R * 6 * X::kRowBytes);
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const long long row = it * R + r;
+#pragma unroll
+      for (int f = 0; f < 6; ++f)
+        bulk_load(stg + (r * 6 + f) * RS, work + (long long)f * g.field + SNS_IDX(row, (long long)N * N) * g.pitch,
+                  X::kRowBytes, bar);
+    }
+  };
+  if (lane == 0 && gw < niter) issue(gw);
+
+  // Four-step twiddles of this lane's j = lane & 15, W_N^(j rr) for the 16 rr it visits
+  // (rr = 2 i + h at N = 512, h = lane >> 4; rr = i at N = 256): from 8 table values,
+  // W^(j (h + S c)) * W^(4 S j a) with i = 4 a + c (S = 2 at N = 512, 1 at N = 256).
+  constexpr int S2 = (N == 512) ? 2 : 1;
+  const int j = lane & 15, hh = (N == 512) ? (lane >> 4) : 0;
+  C twP[4], twQ[4];
+#pragma unroll
+  for (int c = 0; c < 4; ++c) twP[c] = tw2_g[SNS_IDX((hh + S2 * c) * 16 + j, N)];
+#pragma unroll
+  for (int a = 0; a < 4; ++a) twQ[a] = tw2_g[SNS_IDX(4 * S2 * a * 16 + j, N)];
+  auto tw = [&](int i) -> C { return i < 4 ? twP[i] : cmul(twP[i & 3], twQ[i >> 2]); };
+
+  bool ok = true;
+  int k = 0;
+  for (long long it = gw; it < niter; it += nw, ++k) {
+    const bool landed = mbar_wait_bounded(bar, (uint32_t)k & 1u);
+    if (!__all_sync(kFull, landed)) {  // the copy of this row group never landed; none other is in flight
+      ok = false;
+      break;
+    }
+
+    // ---- inverse stage A: lane (t, r), the three components in turn
+    {
+      const int t = lane % M, r = lane / M;
+#pragma unroll 1
+      for (int c = 0; c < 3; ++c) {
+        const C* Ur = stg + (r * 6 + 2 * c) * RS;
+        const C* Vr = Ur + RS;
+        C v[16];
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+          const int x = t + M * q;
+          C z;
+          if (x == 0) {
+            z = cmk(Ur[0].x, Vr[0].x);
+          } else if (x < NH) {
+            const C U = Ur[SNS_IDX(x, RS)], V = Vr[SNS_IDX(x, RS)];
+            z = cmk(U.x - V.y, U.y + V.x);
+          } else if (x == NH) {
+            C U, V;
+            if (nyq_scalar) {
+              U = cscale(unyq[(long long)c * g.field + NH], (float)scale);
+              V = cmul(U, phase[NH + 3 * N / 2]);
+            } else {
+              U = Ur[NH];
+              V = Vr[NH];
+            }
+            z = cmk(U.x, V.x);
+          } else {
+            const C U = Ur[SNS_IDX(N - x, RS)], V = Vr[SNS_IDX(N - x, RS)];
+            z = cmk(U.x + V.y, V.x - U.y);
+          }
+          v[q] = z;
+        }
+        dft16<+1, C, true>(v);
+        C* W = Wc + (r * 3 + c) * N;
+#pragma unroll
+        for (int q = 0; q < 16; ++q) W[SNS_IDX(16 * t + (q ^ (t & 15)), N)] = v[q];
+      }
+    }
+    // the staged rows are consumed: order those reads before the bulk copy of the next row
+    // group into the same buffer, which lands while this group is finished
+    fence_proxy_async_smem();
+    __syncwarp();
+    if (lane == 0 && it + nw < niter) issue(it + nw);
+
+    // ---- inverse stage B: z[c][q] = z_c(j + 16 n), n = q + 16 h (N = 512) or n = q (N = 256)
+    C z[3][16];
+    const int rB = (N == 512) ? 0 : (lane >> 4);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const C* W = Wc + (rB * 3 + c) * N;
+      C v[16];
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        const int rr = S2 * i + hh;  // the stage-A lane t whose output k = j this is
+        v[i] = cmulc(W[SNS_IDX(16 * rr + (j ^ (rr & 15)), N)], tw(i));  // inverse twiddle = conj
+      }
+      dft16<+1, C, true>(v);
+      if constexpr (N == 512) {
+        if (hh) {
+#pragma unroll
+          for (int q = 1; q < 16; ++q) v[q] = cmulc(v[q], w32<C>(q));  // conj W32^q
+        }
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+          const C o = shfl2_xor(v[q], 16);
+          z[c][q] = hh ? psub(o, v[q]) : padd(v[q], o);
+        }
+      } else {
+#pragma unroll
+        for (int q = 0; q < 16; ++q) z[c][q] = v[q];
+      }
+    }
+    __syncwarp();  // Wc is read; the products overwrite it
+
+#pragma unroll
+    for (int half = 0; half < 2; ++half) {
+      // ---- products and forward stage A: P[ab % 3][j][k1] in Wc at 32 j + (k1 ^ j)
+      // (N = 512) or 16 j + (k1 ^ j) (N = 256)
+#pragma unroll
+      for (int ab = 3 * half; ab < 3 * half + 3; ++ab) {
+        // pairs 00 01 02 11 12 22
+        const int ca = (ab >= 3) + (ab >= 5), cb = ab < 3 ? ab : (ab < 5 ? ab - 2 : 2);
+        C v[16];
+#pragma unroll
+        for (int q = 0; q < 16; ++q) v[q] = cmk(z[ca][q].x * z[cb][q].x, z[ca][q].y * z[cb][q].y);
+        if constexpr (N == 512) {
+          // M = 32 split in frequency: h = 0 takes p(n) + p(n + 16) (even k1), h = 1 takes
+          // (p(n) - p(n + 16)) W32^n (odd k1)
+#pragma unroll
+          for (int q = 0; q < 16; ++q) {
+            const C o = shfl2_xor(v[q], 16);
+            v[q] = hh ? (q == 0 ? psub(o, v[q]) : cmul(psub(o, v[q]), w32<C>(q))) : padd(v[q], o);
+          }
+        }
+        dft16<-1, C, true>(v);
+        C* Pab = Wc + ((ab % 3) * R + rB) * N;
+#pragma unroll
+        for (int m = 0; m < 16; ++m) {
+          const int k1 = S2 * m + hh;
+          Pab[SNS_IDX(M * j + (k1 ^ j), N)] = cmul(v[m], tw(m));  // four-step twiddle W_N^(j k1)
+        }
+      }
+      __syncwarp();
+
+      // ---- forward stage B, r2c unpack through the partner lane, stores to HBM
+      {
+        const int k1 = lane % M, r = lane / M;
+        const int partner = (N == 512) ? ((32 - lane) & 31) : ((lane & 16) + ((16 - k1) & 15));
+        const long long row = it * R + r;
+#pragma unroll 1
+        for (int ab = 3 * half; ab < 3 * half + 3; ++ab) {
+          const C* Pab = Wc + ((ab % 3) * R + r) * N;
+          C v[16];
+#pragma unroll
+          for (int jj = 0; jj < 16; ++jj) v[jj] = Pab[SNS_IDX(M * jj + (k1 ^ jj), N)];
+          dft16<-1, C, true>(v);  // v[i] = X(k1 + M i)
+          C* o0 = work + (long long)(2 * ab) * g.field + row * g.pitch;
+          C* o1 = o0 + g.field;
+#pragma unroll
+          for (int i = 0; i < 16; ++i) {
+            const C send = k1 == 0 ? v[(16 - i) & 15] : v[15 - i];
+            const C zm = shfl2(send, partner);  // X(N - k1 - M i)
+            const int kk = k1 + M * i;
+            if (kk <= NH) {
+              C A, B;
+              unpack_pair(v[i], zm, &A, &B);
+              o0[SNS_IDX(kk, g.pitch)] = A;
+              o1[SNS_IDX(kk, g.pitch)] = B;
+              if (kk == NH) {
+                my_nyq[r * 12 + 2 * ab] += A.x;
+                my_nyq[r * 12 + 2 * ab + 1] += B.x;
+              }
+            }
+          }
+        }
+      }
+      __syncwarp();  // Wc is read; the next half (or the next row group) overwrites it
+    }
+  }
+  if (!ok && lane == 0) atomicExch(err, kErrTmaTimeout);
+  // per-CTA Nyquist partials, fixed order: [field][cta]
+  __syncthreads();
+  if (tid < 12) {
+    double s = 0.0;
+#pragma unroll 1
+    for (int w = 0; w < X::WARPS * R; ++w) s += s_nyq[w * 12 + tid];
+    nyq_part[tid * gridDim.x + blockIdx.x] = s;
   }
 }
 
@@ -1907,7 +2160,10 @@ struct Launch {
   }
   static void xpass2(void* work, const void* unyq, const void* phase, double scale, int nyq_scalar, double* nyq_part,
                      const void* tw2, Geom g, int grid, int* err, cudaStream_t st) {
-    if constexpr (N == 256 || N == 512) {
+    if constexpr ((N == 256 || N == 512) && std::is_same_v<C, float2>) {
+      k_xpass_w<N><<<grid, 32 * XW<N>::WARPS, XW<N>::smem, st>>>(F(work), F(unyq), F(phase), scale, nyq_scalar,
+                                                                 nyq_part, F(tw2), g, err);
+    } else if constexpr (N == 256 || N == 512) {
       k_xpass2<N, C><<<grid, XP<N, C>::NT, XP<N, C>::smem, st>>>(F(work), F(unyq), F(phase), scale, nyq_scalar,
                                                                   nyq_part, F(tw2), g, err);
     }
@@ -1949,7 +2205,14 @@ struct Launch {
   }
   // Persistent grid of the two-stage x pass (0: this size uses the generic x pass).
   static int xpass2_grid(int nsm) {
-    if constexpr (N == 256 || N == 512) {
+    if constexpr ((N == 256 || N == 512) && std::is_same_v<C, float2>) {
+      int nb = 0;
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_xpass_w<N>, 32 * XW<N>::WARPS, XW<N>::smem);
+      // every warp owns row groups: no CTA beyond one per XW::WARPS row groups
+      const long long ncta = ((long long)N * N / XW<N>::R + XW<N>::WARPS - 1) / XW<N>::WARPS;
+      long long grid = (long long)nsm * (nb > 0 ? nb : 1);
+      return (int)(grid < ncta ? grid : ncta);
+    } else if constexpr (N == 256 || N == 512) {
       int nb = 0;
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_xpass2<N, C>, XP<N, C>::NT, XP<N, C>::smem);
       const long long niter = (long long)N * N / XP<N, C>::ROWS;
@@ -2015,7 +2278,8 @@ struct Launch {
   }
   // Opt every kernel of this size into its dynamic shared memory (once per process).
   static void init() {
-    if constexpr (N == 256 || N == 512) set_smem(k_xpass2<N, C>, XP<N, C>::smem);
+    if constexpr ((N == 256 || N == 512) && std::is_same_v<C, float2>) set_smem(k_xpass_w<N>, XW<N>::smem);
+    else if constexpr (N == 256 || N == 512) set_smem(k_xpass2<N, C>, XP<N, C>::smem);
     if constexpr (N == 128 || N == 256 || N == 512) set_smem(k_p5<N, C>, tma_smem<N, C>());
     set_smem(k_yz_tma<N, 2, +1, 1, C>, tma_smem<N, C>());
     set_smem(k_yz_tma<N, 1, -1, 0, C>, tma_smem<N, C>());
