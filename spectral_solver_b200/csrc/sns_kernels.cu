@@ -791,8 +791,9 @@ struct XW {
   static constexpr int WC = R * 3 * N;    // transposition buffer [R][3][N]
   static constexpr int PER_WARP = STG + WC;
   static constexpr uint32_t kRowBytes = RS * sizeof(C);
-  static constexpr size_t smem =
-      (size_t)WARPS * PER_WARP * sizeof(C) + 128 + WARPS * (sizeof(uint64_t) + R * 12 * sizeof(double));
+  static constexpr int TWT = 16 * 32;     // four-step twiddles [i][lane]
+  static constexpr size_t smem = (size_t)(WARPS * PER_WARP + TWT) * sizeof(C) + 128 +
+                                 WARPS * (sizeof(uint64_t) + R * 12 * sizeof(double));
   static_assert(R * M == 32, "a warp covers its rows' lanes");
 };
 
@@ -810,9 +811,9 @@ k_xpass_w(float2* __restrict__ work, const float2* __restrict__ unyq, const floa
   C* const all = reinterpret_cast<C*>(smraw + pad);
   C* const stg = all + warp * X::PER_WARP;  // [R][6][RS]
   C* const Wc = stg + X::STG;               // [R][3][N], element (t, k) at 16 t + (k ^ (t & 15))
-  uint64_t* const bar = reinterpret_cast<uint64_t*>(all + X::WARPS * X::PER_WARP) + warp;
-  double* const s_nyq =
-      reinterpret_cast<double*>(reinterpret_cast<uint64_t*>(all + X::WARPS * X::PER_WARP) + X::WARPS);
+  C* const twt = all + X::WARPS * X::PER_WARP;  // [16][32]
+  uint64_t* const bar = reinterpret_cast<uint64_t*>(twt + X::TWT) + warp;
+  double* const s_nyq = reinterpret_cast<double*>(reinterpret_cast<uint64_t*>(twt + X::TWT) + X::WARPS);
   double* const my_nyq = s_nyq + warp * R * 12;  // [WARPS][R][12]
   if (lane < R * 12) my_nyq[lane] = 0.0;
   if (lane == 0) {
@@ -835,17 +836,17 @@ k_xpass_w(float2* __restrict__ work, const float2* __restrict__ unyq, const floa
   };
   if (lane == 0 && gw < niter) issue(gw);
 
-  // Four-step twiddles of this lane's j = lane & 15, W_N^(j rr) for the 16 rr it visits
-  // (rr = 2 i + h at N = 512, h = lane >> 4; rr = i at N = 256): from 8 table values,
-  // W^(j (h + S c)) * W^(4 S j a) with i = 4 a + c (S = 2 at N = 512, 1 at N = 256).
+  // Four-step twiddles: lane L (j = L & 15, h = L >> 4 at N = 512) visits rr = 2 i + h at
+  // N = 512, rr = i at N = 256, and needs W_N^(j rr) = tw2[rr][j]; the CTA keeps them as
+  // twt[i][L] (one table for every warp; consecutive lanes, consecutive words).
   constexpr int S2 = (N == 512) ? 2 : 1;
   const int j = lane & 15, hh = (N == 512) ? (lane >> 4) : 0;
-  C twP[4], twQ[4];
-#pragma unroll
-  for (int c = 0; c < 4; ++c) twP[c] = tw2_g[SNS_IDX((hh + S2 * c) * 16 + j, N)];
-#pragma unroll
-  for (int a = 0; a < 4; ++a) twQ[a] = tw2_g[SNS_IDX(4 * S2 * a * 16 + j, N)];
-  auto tw = [&](int i) -> C { return i < 4 ? twP[i] : cmul(twP[i & 3], twQ[i >> 2]); };
+  for (int e = tid; e < X::TWT; e += 32 * X::WARPS) {
+    const int i = e >> 5, L = e & 31;
+    twt[e] = tw2_g[SNS_IDX((S2 * i + ((N == 512) ? (L >> 4) : 0)) * 16 + (L & 15), N)];
+  }
+  __syncthreads();
+  auto tw = [&](int i) -> C { return twt[SNS_IDX(i * 32 + lane, X::TWT)]; };
 
   bool ok = true;
   int k = 0;
@@ -866,14 +867,15 @@ k_xpass_w(float2* __restrict__ work, const float2* __restrict__ unyq, const floa
         C v[16];
 #pragma unroll
         for (int q = 0; q < 16; ++q) {
+          // x = t + M q: below N/2 for q < 8, N/2 + t for q = 8, above N/2 for q > 8
           const int x = t + M * q;
           C z;
-          if (x == 0) {
+          if (q == 0 && t == 0) {
             z = cmk(Ur[0].x, Vr[0].x);
-          } else if (x < NH) {
+          } else if (q < 8) {
             const C U = Ur[SNS_IDX(x, RS)], V = Vr[SNS_IDX(x, RS)];
             z = cmk(U.x - V.y, U.y + V.x);
-          } else if (x == NH) {
+          } else if (q == 8 && t == 0) {
             C U, V;
             if (nyq_scalar) {
               U = cscale(unyq[(long long)c * g.field + NH], (float)scale);
@@ -975,8 +977,9 @@ k_xpass_w(float2* __restrict__ work, const float2* __restrict__ unyq, const floa
           dft16<-1, C, true>(v);  // v[i] = X(k1 + M i)
           C* o0 = work + (long long)(2 * ab) * g.field + row * g.pitch;
           C* o1 = o0 + g.field;
+          // outputs k = k1 + M i <= N/2 only: i <= 8 (i = 8 is the Nyquist column, lane k1 = 0)
 #pragma unroll
-          for (int i = 0; i < 16; ++i) {
+          for (int i = 0; i <= NH / M; ++i) {
             const C send = k1 == 0 ? v[(16 - i) & 15] : v[15 - i];
             const C zm = shfl2(send, partner);  // X(N - k1 - M i)
             const int kk = k1 + M * i;
@@ -2373,8 +2376,7 @@ void launch_spectral_diag(const void* u, int precision, double* partials, int nb
 }
 // One thread: the reference's adaptive step (run_taylor_green, ava_taylor_green_impl.hpp:
 // 1363-1378) on the device, with the horizon in place of the output times.
-__global__ void k_clock_step(const double* __restrict__ vmax2, double* __restrict__ c) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+__device__ void clock_advance(const double* __restrict__ vmax2, double* __restrict__ c) {
   const double t = c[kClockT], t_end = c[kClockTEnd];
   if (c[kClockStopped] != 0.0 || !(t < t_end - 1.0e-14)) {
     c[kClockStopped] = 1.0;
@@ -2388,6 +2390,9 @@ __global__ void k_clock_step(const double* __restrict__ vmax2, double* __restric
   c[kClockDt] = dt;
   c[kClockT] = t + dt;
   c[kClockSteps] += 1.0;
+}
+__global__ void k_clock_step(const double* __restrict__ vmax2, double* __restrict__ c) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) clock_advance(vmax2, c);
 }
 
 // The index-check record of the debug build: {count, first line, first index}; count -1 in
@@ -2410,6 +2415,26 @@ int bounds_record(long long* out3) {
 
 void launch_clock_step(const double* vmax2, double* clock, cudaStream_t st) {
   k_clock_step<<<1, 32, 0, st>>>(vmax2, clock);
+}
+
+// The max of the per-row vmax^2 partials (as k_reduce: max is exact in any order) and the
+// clock's step from it in one launch, for the device CFL step.
+__global__ void __launch_bounds__(256) k_clock_step_partials(const double* __restrict__ partials, int count,
+                                                             int stride, double* __restrict__ c) {
+  __shared__ double red[256];
+  double m = 0.0;
+  for (int i = threadIdx.x; i < count; i += 256) m = fmax(m, partials[(long long)i * stride]);
+  red[threadIdx.x] = m;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if (threadIdx.x < o) red[threadIdx.x] = fmax(red[threadIdx.x], red[threadIdx.x + o]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) clock_advance(red, c);
+}
+
+void launch_clock_step_partials(const double* partials, int count, int stride, double* clock, cudaStream_t st) {
+  k_clock_step_partials<<<1, 256, 0, st>>>(partials, count, stride, clock);
 }
 
 void launch_reduce(const double* partials, int count, int stride, int op_max, double* out, cudaStream_t st) {

@@ -146,6 +146,7 @@ void launch_reduce(const double* partials, int count, int stride, int op_max, do
 // ava_taylor_green_impl.hpp:1363-1368): dt = min(dt_max, cfl dx / vmax), clipped to the
 // horizon; stops the clock at the horizon; advances t and the step count.
 void launch_clock_step(const double* vmax2, double* clock, cudaStream_t st);
+void launch_clock_step_partials(const double* partials, int count, int stride, double* clock, cudaStream_t st);
 // the index-check record of the debug build (count -1 without checks); a cudaError_t or 0
 int bounds_record(long long* out3);
 
