@@ -82,7 +82,7 @@ TRAFFIC_PER_POINT = {"p5_sweep": (16.716e9 + 5.166e9) / 512 ** 3, "p3_xpass": (6
                      "p4_yfwd": 3.268e9 / 256 ** 3, "p1_zinv_phase": 1.166e9 / 256 ** 3,
                      "p2_yinv": 1.582e9 / 256 ** 3}
 # The same for the FP32 precision form.
-TRAFFIC_PER_POINT_FP32 = {"p3_xpass": (3.474e9 + 6.487e9) / 512 ** 3, "p5_sweep": (8.473e9 + 2.619e9) / 512 ** 3}
+TRAFFIC_PER_POINT_FP32 = {"p3_xpass": (3.485e9 + 6.485e9) / 512 ** 3, "p5_sweep": (9.059e9 + 2.983e9) / 512 ** 3}
 
 
 def load_peaks():
@@ -385,7 +385,8 @@ def e2e_solve(args, s, n, pg):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     units = world * n ** 3 * args.steps
     return {"value": units / e2e_s / 1e9, "unit": UNIT,
-            "h2d_bytes_per_step": 3 * 2 * n ** 3 * 8 / args.steps,
+            # set_state copies columns 0..N/2 of each row of the full-layout spectrum
+            "h2d_bytes_per_step": 3 * n * n * (n // 2 + 1) * 16 / args.steps,
             "d2h_bytes_per_step": (3 * n ** 3 * 8 + args.steps * 6 * 8) / args.steps,
             "what": "set_state from pinned host + K x (step + diagnostics row to host) + final velocity to host"}
 

@@ -1974,7 +1974,7 @@ __global__ void k_half_to_full(const C* __restrict__ half, double2* __restrict__
 // (c_m + conj(c_-m))/2 is stored, so a c2r of the result equals Re(IDFT(c)).
 template <class C>
 __global__ void k_full_to_half(const double2* __restrict__ full, C* __restrict__ half, int hermitian_part,
-                               Geom g, CompWord* __restrict__ lo) {
+                               long long src_pitch, Geom g, CompWord* __restrict__ lo) {
   const long long n = g.n;
   const long long total = n * n * (g.nh + 1);
   const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -1982,8 +1982,8 @@ __global__ void k_full_to_half(const double2* __restrict__ full, C* __restrict__
   const long long row = e / (g.nh + 1);
   const int x = (int)(e % (g.nh + 1));
   const long long y = row % n, z = row / n;
-  double2 v = full[(z * n + y) * n + x];
-  if (hermitian_part) {
+  double2 v = full[row * src_pitch + x];  // src_pitch n: the full layout; nh + 1: its left half
+  if (hermitian_part) {  // (full layout only)
     const long long ym = (n - y) % n, zm = (n - z) % n, xm = (n - x) % n;
     const double2 w = full[(zm * n + ym) * n + xm];
     v = make_double2(0.5 * (v.x + w.x), 0.5 * (v.y - w.y));
@@ -2362,13 +2362,15 @@ void launch_half_to_full(const void* half, int precision, double2* full, Geom g,
   else k_half_to_full<float2><<<blocks_for(total, 256), 256, 0, st>>>(FC<float2>(half), full, g, lo);
 }
 void launch_full_to_half(const double2* full, void* half, int precision, int hermitian_part, Geom g,
-                         cudaStream_t st, CompWord* lo) {
+                         cudaStream_t st, CompWord* lo, long long src_pitch) {
   const long long total = (long long)g.n * g.n * (g.nh + 1);
+  if (src_pitch <= 0 || hermitian_part) src_pitch = g.n;
   if (precision == 0)
-    k_full_to_half<double2><<<blocks_for(total, 256), 256, 0, st>>>(full, FC<double2>(half), hermitian_part, g,
-                                                                      nullptr);
+    k_full_to_half<double2><<<blocks_for(total, 256), 256, 0, st>>>(full, FC<double2>(half), hermitian_part,
+                                                                      src_pitch, g, nullptr);
   else
-    k_full_to_half<float2><<<blocks_for(total, 256), 256, 0, st>>>(full, FC<float2>(half), hermitian_part, g, lo);
+    k_full_to_half<float2><<<blocks_for(total, 256), 256, 0, st>>>(full, FC<float2>(half), hermitian_part,
+                                                                    src_pitch, g, lo);
 }
 void launch_spectral_diag(const void* u, int precision, double* partials, int nblocks, Geom g, cudaStream_t st) {
   if (precision == 0) k_spectral_diag<double2><<<nblocks, 256, 0, st>>>(FC<double2>(u), partials, g);

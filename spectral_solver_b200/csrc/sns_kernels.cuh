@@ -138,8 +138,10 @@ void launch_add_sparse(void* u, int precision, const long long* idx, const doubl
 // half_to_full adds them, full_to_half writes the remainder the FP32 value drops
 void launch_half_to_full(const void* half, int precision, double2* full, Geom g, cudaStream_t st,
                          const CompWord* lo = nullptr);
+// src_pitch: complex values between rows of `full` (0: n, the full layout; n/2 + 1 when only
+// the left half of each row was staged, which is all the plain conversion reads)
 void launch_full_to_half(const double2* full, void* half, int precision, int hermitian_part, Geom g,
-                         cudaStream_t st, CompWord* lo = nullptr);
+                         cudaStream_t st, CompWord* lo = nullptr, long long src_pitch = 0);
 void launch_spectral_diag(const void* u, int precision, double* partials, int nblocks, Geom g, cudaStream_t st);
 void launch_reduce(const double* partials, int count, int stride, int op_max, double* out, cudaStream_t st);
 // The next step of a device clock from vmax^2 (the reference's adaptive rule,

@@ -141,7 +141,8 @@ int batch_finish(sns_batch* b, const char* what) {
 // (its state re-initialised in place), so a steady stream admits and retires without
 // cudaMalloc or cudaFree, which would synchronise the whole device.  The budget counts
 // resident and idle handles; an idle handle of another N is freed only when a request needs
-// its room.
+// its room and no solve of the request's N is resident (else the request waits for that
+// handle, and queued requests with an idle handle start in the meantime).
 // Time: a tick never waits for GPU work.  It queues a resident solve's next batch of steps
 // only when at most one earlier batch is still in flight (two batches queued per solve keep
 // the device busy between ticks); each batch ends with a copy of the clock to pinned host
@@ -259,7 +260,53 @@ int make_slot(sns_server* s, const sns_request& q, size_t bytes, sns_server::Slo
   return SNS_OK;
 }
 
-// Admit queued requests in arrival order while their device bytes fit the budget.
+// Start request p on an idle handle of its N (re-initialised in place, no allocation) or on
+// a new handle `fresh`; false with the error set if the handle cannot take it.
+int start_request(sns_server* s, const sns_server::Pending& p, sns_server::Slot slot, bool fresh) {
+  sns_server::Resident r;
+  r.id = p.id;
+  r.req = p.req;
+  r.slot = slot;
+  int rc = SNS_OK;
+  std::string err;
+  if (!fresh) {
+    rc = sns::reset_handle(r.slot.h, p.req.nu, p.req.seed, p.req.pert_amp, p.req.pert_kmax);
+    if (rc != SNS_OK) err = sns_last_error(r.slot.h);
+  }
+  if (rc == SNS_OK) {
+    rc = sns_set_clock(r.slot.h, 0.0, p.req.t_end, p.req.cfl, p.req.dt_max);
+    if (rc != SNS_OK) err = sns_last_error(r.slot.h);
+  }
+  if (rc != SNS_OK) {
+    free_slot(r.slot);
+    return server_fail(s, rc, "request " + std::to_string(p.id) + ": " + err);
+  }
+  s->used += r.slot.bytes;
+  s->resident.push_back(r);
+  return SNS_OK;
+}
+
+// The idle handle of size n, taken out of the pool (false if there is none).
+bool take_idle(sns_server* s, int n, sns_server::Slot* out) {
+  for (size_t k = 0; k < s->idle.size(); ++k)
+    if (s->idle[k].n == n) {
+      *out = s->idle[k];
+      s->idle.erase(s->idle.begin() + (long)k);
+      s->idle_bytes -= out->bytes;
+      return true;
+    }
+  return false;
+}
+
+// Queued requests behind a waiting head that may start on an idle handle meanwhile.
+constexpr size_t kLookahead = 64;
+
+// Admit queued requests in arrival order while their device bytes fit the budget.  The head
+// request takes an idle handle of its N, else unused budget, else -- when no solve of its N
+// is resident -- the room of idle handles of other sizes (freed).  When a solve of its N is
+// resident, the head waits for that handle instead of freeing and allocating (cudaFree and
+// cudaMalloc synchronise the device), and requests behind it whose N has an idle handle
+// start meanwhile, so the pool's memory keeps working.
 int admit(sns_server* s) {
   while (!s->queue.empty()) {
     const sns_server::Pending p = s->queue.front();
@@ -271,38 +318,42 @@ int admit(sns_server* s) {
     if (bytes > s->budget)
       return server_fail(s, SNS_ERR_NOMEM, "request " + std::to_string(p.id) + " needs " + std::to_string(bytes) +
                                                " bytes, more than the whole HBM budget");
-    sns_server::Resident r;
-    r.id = p.id;
-    r.req = p.req;
-    size_t k = 0;
-    while (k < s->idle.size() && s->idle[k].n != p.req.n) ++k;
-    int rc = SNS_OK;
+    sns_server::Slot slot;
+    if (take_idle(s, p.req.n, &slot)) {
+      s->queue.pop_front();
+      const int rc = start_request(s, p, slot, false);
+      if (rc != SNS_OK) return rc;
+      continue;
+    }
+    const bool unused_room = s->used + s->idle_bytes + bytes <= s->budget;
+    bool same_n_resident = false;
+    for (const sns_server::Resident& r : s->resident) same_n_resident = same_n_resident || r.req.n == p.req.n;
+    if (!unused_room && same_n_resident) {
+      // the head waits for a handle of its N; later requests with an idle handle start now
+      for (size_t q = 1; q < s->queue.size() && q <= kLookahead && !s->idle.empty();) {
+        const sns_server::Pending pq = s->queue[q];
+        if (take_idle(s, pq.req.n, &slot)) {
+          s->queue.erase(s->queue.begin() + (long)q);
+          const int rc = start_request(s, pq, slot, false);
+          if (rc != SNS_OK) return rc;
+        } else {
+          ++q;
+        }
+      }
+      return SNS_OK;
+    }
+    if (!make_room(s, bytes)) return SNS_OK;  // waits until retirements free memory
     std::string err;
-    if (k < s->idle.size()) {
-      // an idle handle of this N: re-initialised in place, no allocation
-      r.slot = s->idle[k];
-      s->idle.erase(s->idle.begin() + (long)k);
-      s->idle_bytes -= r.slot.bytes;
-      rc = sns::reset_handle(r.slot.h, p.req.nu, p.req.seed, p.req.pert_amp, p.req.pert_kmax);
-      if (rc != SNS_OK) err = sns_last_error(r.slot.h);
-    } else {
-      if (!make_room(s, bytes)) return SNS_OK;  // waits until retirements free memory
-      rc = make_slot(s, p.req, bytes, &r.slot, &err);
-      if (rc == SNS_ERR_NOMEM && !s->resident.empty()) return SNS_OK;  // the device itself is full: wait
-      if (rc == SNS_OK) ++s->allocations;
-    }
-    if (rc == SNS_OK) {
-      rc = sns_set_clock(r.slot.h, 0.0, p.req.t_end, p.req.cfl, p.req.dt_max);
-      if (rc != SNS_OK) err = sns_last_error(r.slot.h);
-    }
+    const int rc = make_slot(s, p.req, bytes, &slot, &err);
+    if (rc == SNS_ERR_NOMEM && !s->resident.empty()) return SNS_OK;  // the device itself is full: wait
     if (rc != SNS_OK) {
-      if (r.slot.h) free_slot(r.slot);
       s->queue.pop_front();
       return server_fail(s, rc, "request " + std::to_string(p.id) + ": " + err);
     }
+    ++s->allocations;
     s->queue.pop_front();
-    s->used += r.slot.bytes;
-    s->resident.push_back(r);
+    const int rc2 = start_request(s, p, slot, true);
+    if (rc2 != SNS_OK) return rc2;
   }
   return SNS_OK;
 }

@@ -173,6 +173,35 @@ def test_server_reuses_retired_handles(mod):
             assert done[i]["final"][key] == alone[0]["final"][key], key
 
 
+def test_server_mixed_sizes_wait_for_their_handles(mod):
+    """Alternating 32^3 and 48^3 requests under a budget of one handle of each: a request
+    whose N has a resident solve waits for that handle instead of freeing the idle handle of
+    the other size and allocating (cudaFree / cudaMalloc synchronise the device), so eight
+    requests are served by the two handles created at the start."""
+    lib = mod.load()
+    per32, per48 = lib.sns_bytes_required(32, FP32), lib.sns_bytes_required(48, FP32)
+    reqs = []
+    for i in range(8):
+        n = 32 if i % 2 == 0 else 48
+        reqs.append(dict(n=n, nu=1 / (400.0 + 50 * i), t_end=0.2 + 0.15 * ((i * 5) % 4), seed=40 + i,
+                         pert_amp=1e-3, pert_kmax=4))
+    budget = per32 + per48
+    done = {}
+    with mod.Server(budget, FP32) as srv:
+        ids = [srv.submit(**r) for r in reqs]
+        for _ in range(400000):
+            out, res, q, used = srv.step()
+            assert used <= budget
+            for r in out:
+                done[r["id"]] = r
+            if len(done) == len(reqs):
+                break
+        stats = srv.stats()
+    assert len(done) == len(reqs)
+    assert stats["handles_created"] == 2
+    assert all(np.isfinite(done[i]["final"]["kinetic_energy"]) for i in ids)
+
+
 @pytest.mark.parametrize("precision", [FP64, FP32])
 def test_device_clock_matches_host_adaptive_loop(mod, precision):
     """sns_step_cfl takes the reference's adaptive step on the device: the same step sizes,
