@@ -94,6 +94,12 @@ __device__ __forceinline__ float2 psub(float2 a, float2 b) {
   asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(f2_pack(a)), "l"(f2_pack(b)));
   return f2_unpack(d);
 }
+// (a.x * b.x, a.y * b.y) in one packed instruction
+__device__ __forceinline__ float2 pmul(float2 a, float2 b) {
+  unsigned long long d;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(f2_pack(a)), "l"(f2_pack(b)));
+  return f2_unpack(d);
+}
 
 // a * conj(b)
 template <class C>

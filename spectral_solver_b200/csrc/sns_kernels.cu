@@ -756,7 +756,7 @@ k_xpass2(C* __restrict__ work, const C* __restrict__ unyq, const C* __restrict__
 }
 
 // ---------------------------------------------------------------------------------------
-// x pass of the FP32 form at N = 256 and 512: one warp owns R = 512 / N rows at a time and
+// x pass of the FP32 form at N = 128, 256 and 512: one warp owns R = 512 / N rows at a time and
 // runs every stage of them alone, so the CTA (eight warps, one CTA per SM) never
 // synchronises inside the loop.  The same operation as k_xpass2 (reference: the nonlinear
 // term of spectral_solver.cpp:93-158, 169-215 on the r2c layout), reorganised so the three
@@ -766,7 +766,8 @@ k_xpass2(C* __restrict__ work, const C* __restrict__ unyq, const C* __restrict__
 //                    The staging buffer is then free: the next row group's bulk copy is
 //                    issued into it and lands while the rest of this group is transformed.
 //   inverse stage B  lane (j, h): the M-point DFT over t at fixed k = j (four-step twiddle
-//                    W_N^(j t) before; at N = 512 two half-warps and one shuffle), leaving
+//                    W_N^(j t) before; at N = 512 two half-warps and one shuffle; at N = 128
+//                    8-point DFTs, a lane taking two of the warp's four rows in turn), leaving
 //                    z_c(x) for x = j + 16 n, n of the lane, of all three components in
 //                    registers
 //   products + forward stage A  per product u_a u_b (both grids: real and imaginary part)
@@ -791,8 +792,8 @@ struct XW {
   static constexpr int WC = R * 3 * N;    // transposition buffer [R][3][N]
   static constexpr int PER_WARP = STG + WC;
   static constexpr uint32_t kRowBytes = RS * sizeof(C);
-  static constexpr int TWT = 16 * 32;     // four-step twiddles [i][lane]
-  static constexpr size_t smem = (size_t)(WARPS * PER_WARP + TWT) * sizeof(C) + 128 +
+  static constexpr int TWT = 16 * 32;     // four-step twiddles [i][lane], then the same halved
+  static constexpr size_t smem = (size_t)(WARPS * PER_WARP + 2 * TWT) * sizeof(C) + 128 +
                                  WARPS * (sizeof(uint64_t) + R * 12 * sizeof(double));
   static_assert(R * M == 32, "a warp covers its rows' lanes");
 };
@@ -812,10 +813,11 @@ k_xpass_w(float2* __restrict__ work, const float2* __restrict__ unyq, const floa
   C* const stg = all + warp * X::PER_WARP;  // [R][6][RS]
   C* const Wc = stg + X::STG;               // [R][3][N], element (t, k) at 16 t + (k ^ (t & 15))
   C* const twt = all + X::WARPS * X::PER_WARP;  // [16][32]
-  uint64_t* const bar = reinterpret_cast<uint64_t*>(twt + X::TWT) + warp;
-  double* const s_nyq = reinterpret_cast<double*>(reinterpret_cast<uint64_t*>(twt + X::TWT) + X::WARPS);
+  C* const twh = twt + X::TWT;                   // [16][32], times 1/2
+  uint64_t* const bar = reinterpret_cast<uint64_t*>(twh + X::TWT) + warp;
+  double* const s_nyq = reinterpret_cast<double*>(reinterpret_cast<uint64_t*>(twh + X::TWT) + X::WARPS);
   double* const my_nyq = s_nyq + warp * R * 12;  // [WARPS][R][12]
-  if (lane < R * 12) my_nyq[lane] = 0.0;
+  for (int e = lane; e < R * 12; e += 32) my_nyq[e] = 0.0;
   if (lane == 0) {
     mbar_init(bar, 1);
     fence_mbar_init();
@@ -838,15 +840,32 @@ k_xpass_w(float2* __restrict__ work, const float2* __restrict__ unyq, const floa
 
   // Four-step twiddles: lane L (j = L & 15, h = L >> 4 at N = 512) visits rr = 2 i + h at
   // N = 512, rr = i at N = 256, and needs W_N^(j rr) = tw2[rr][j]; the CTA keeps them as
-  // twt[i][L] (one table for every warp; consecutive lanes, consecutive words).
+  // twt[i][L] (one table for every warp; consecutive lanes, consecutive words).  The forward
+  // stage takes them halved (twh, exact): the r2c unpack's factor 1/2 rides on the twiddle
+  // multiply that is there anyway, with bitwise the same results.
   constexpr int S2 = (N == 512) ? 2 : 1;
   const int j = lane & 15, hh = (N == 512) ? (lane >> 4) : 0;
   for (int e = tid; e < X::TWT; e += 32 * X::WARPS) {
     const int i = e >> 5, L = e & 31;
-    twt[e] = tw2_g[SNS_IDX((S2 * i + ((N == 512) ? (L >> 4) : 0)) * 16 + (L & 15), N)];
+    const int rr = S2 * i + ((N == 512) ? (L >> 4) : 0);
+    const C w = rr < M ? tw2_g[SNS_IDX(rr * 16 + (L & 15), N)] : cmk(0.f, 0.f);  // (N = 128: i < 8)
+    twt[e] = w;
+    twh[e] = cmk(0.5f * w.x, 0.5f * w.y);
   }
   __syncthreads();
   auto tw = [&](int i) -> C { return twt[SNS_IDX(i * 32 + lane, X::TWT)]; };
+  auto twhalf = [&](int i) -> C { return twh[SNS_IDX(i * 32 + lane, X::TWT)]; };
+  // Swizzles.  Wc: element (t, k) of a row at 16 t + (k ^ key); P: element (j, k1) of a row
+  // and product at pslot.  At N = 128 a half-warp spans two rows, so the row enters both.
+  auto wkey = [](int t, int r) { return N == 128 ? ((t + 8 * (r & 1)) & 15) : (t & 15); };
+  auto pslot = [](int jr, int k1, int r) {
+    if constexpr (N == 128) {
+      const int jj = jr ^ (r & 1);
+      return 8 * jj + (k1 ^ ((jj >> 1) & 7));
+    } else {
+      return M * jr + (k1 ^ jr);
+    }
+  };
 
   bool ok = true;
   int k = 0;
@@ -894,7 +913,7 @@ k_xpass_w(float2* __restrict__ work, const float2* __restrict__ unyq, const floa
         dft16<+1, C, true>(v);
         C* W = Wc + (r * 3 + c) * N;
 #pragma unroll
-        for (int q = 0; q < 16; ++q) W[SNS_IDX(16 * t + (q ^ (t & 15)), N)] = v[q];
+        for (int q = 0; q < 16; ++q) W[SNS_IDX(16 * t + (q ^ wkey(t, r)), N)] = v[q];
       }
     }
     // the staged rows are consumed: order those reads before the bulk copy of the next row
@@ -903,62 +922,80 @@ k_xpass_w(float2* __restrict__ work, const float2* __restrict__ unyq, const floa
     __syncwarp();
     if (lane == 0 && it + nw < niter) issue(it + nw);
 
-    // ---- inverse stage B: z[c][q] = z_c(j + 16 n), n = q + 16 h (N = 512) or n = q (N = 256)
-    C z[3][16];
-    const int rB = (N == 512) ? 0 : (lane >> 4);
+    // ---- inverse stage B: z[p][c][q] = z_c(j + 16 n) of row rB(p), n = q + 16 h (N = 512),
+    // n = q (N = 256, 128); at N = 128 (M = 8) a lane takes two rows in turn (p = 0, 1)
+    constexpr int MP = (N == 128) ? 2 : 1;
+    constexpr int NZ = 16 / MP;  // positions per lane and row
+    auto row_b = [&](int p) { return N == 512 ? 0 : (N == 256 ? (lane >> 4) : 2 * p + (lane >> 4)); };
+    C z[MP][3][NZ];
 #pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      const C* W = Wc + (rB * 3 + c) * N;
-      C v[16];
+    for (int p = 0; p < MP; ++p) {
+      const int rB = row_b(p);
 #pragma unroll
-      for (int i = 0; i < 16; ++i) {
-        const int rr = S2 * i + hh;  // the stage-A lane t whose output k = j this is
-        v[i] = cmulc(W[SNS_IDX(16 * rr + (j ^ (rr & 15)), N)], tw(i));  // inverse twiddle = conj
-      }
-      dft16<+1, C, true>(v);
-      if constexpr (N == 512) {
-        if (hh) {
+      for (int c = 0; c < 3; ++c) {
+        const C* W = Wc + (rB * 3 + c) * N;
+        C v[NZ];
 #pragma unroll
-          for (int q = 1; q < 16; ++q) v[q] = cmulc(v[q], w32<C>(q));  // conj W32^q
+        for (int i = 0; i < NZ; ++i) {
+          const int rr = S2 * i + hh;  // the stage-A lane t whose output k = j this is
+          v[i] = cmulc(W[SNS_IDX(16 * rr + (j ^ wkey(rr, rB)), N)], tw(i));  // inverse twiddle = conj
         }
-#pragma unroll
-        for (int q = 0; q < 16; ++q) {
-          const C o = shfl2_xor(v[q], 16);
-          z[c][q] = hh ? psub(o, v[q]) : padd(v[q], o);
+        if constexpr (N == 128) {
+          dft8<+1>(v);
+        } else {
+          dft16<+1, C, true>(v);
         }
-      } else {
+        if constexpr (N == 512) {
+          if (hh) {
 #pragma unroll
-        for (int q = 0; q < 16; ++q) z[c][q] = v[q];
+            for (int q = 1; q < 16; ++q) v[q] = cmulc(v[q], w32<C>(q));  // conj W32^q
+          }
+#pragma unroll
+          for (int q = 0; q < 16; ++q) {
+            const C o = shfl2_xor(v[q], 16);
+            z[p][c][q] = hh ? psub(o, v[q]) : padd(v[q], o);
+          }
+        } else {
+#pragma unroll
+          for (int q = 0; q < NZ; ++q) z[p][c][q] = v[q];
+        }
       }
     }
     __syncwarp();  // Wc is read; the products overwrite it
 
 #pragma unroll
     for (int half = 0; half < 2; ++half) {
-      // ---- products and forward stage A: P[ab % 3][j][k1] in Wc at 32 j + (k1 ^ j)
-      // (N = 512) or 16 j + (k1 ^ j) (N = 256)
+      // ---- products and forward stage A: P[ab % 3][j][k1] in Wc at pslot(j, k1, row)
 #pragma unroll
-      for (int ab = 3 * half; ab < 3 * half + 3; ++ab) {
-        // pairs 00 01 02 11 12 22
-        const int ca = (ab >= 3) + (ab >= 5), cb = ab < 3 ? ab : (ab < 5 ? ab - 2 : 2);
-        C v[16];
+      for (int p = 0; p < MP; ++p) {
+        const int rB = row_b(p);
 #pragma unroll
-        for (int q = 0; q < 16; ++q) v[q] = cmk(z[ca][q].x * z[cb][q].x, z[ca][q].y * z[cb][q].y);
-        if constexpr (N == 512) {
-          // M = 32 split in frequency: h = 0 takes p(n) + p(n + 16) (even k1), h = 1 takes
-          // (p(n) - p(n + 16)) W32^n (odd k1)
+        for (int ab = 3 * half; ab < 3 * half + 3; ++ab) {
+          // pairs 00 01 02 11 12 22
+          const int ca = (ab >= 3) + (ab >= 5), cb = ab < 3 ? ab : (ab < 5 ? ab - 2 : 2);
+          C v[NZ];
 #pragma unroll
-          for (int q = 0; q < 16; ++q) {
-            const C o = shfl2_xor(v[q], 16);
-            v[q] = hh ? (q == 0 ? psub(o, v[q]) : cmul(psub(o, v[q]), w32<C>(q))) : padd(v[q], o);
+          for (int q = 0; q < NZ; ++q) v[q] = pmul(z[p][ca][q], z[p][cb][q]);
+          if constexpr (N == 512) {
+            // M = 32 split in frequency: h = 0 takes p(n) + p(n + 16) (even k1), h = 1 takes
+            // (p(n) - p(n + 16)) W32^n (odd k1)
+#pragma unroll
+            for (int q = 0; q < 16; ++q) {
+              const C o = shfl2_xor(v[q], 16);
+              v[q] = hh ? (q == 0 ? psub(o, v[q]) : cmul(psub(o, v[q]), w32<C>(q))) : padd(v[q], o);
+            }
           }
-        }
-        dft16<-1, C, true>(v);
-        C* Pab = Wc + ((ab % 3) * R + rB) * N;
+          if constexpr (N == 128) {
+            dft8<-1>(v);
+          } else {
+            dft16<-1, C, true>(v);
+          }
+          C* Pab = Wc + ((ab % 3) * R + rB) * N;
 #pragma unroll
-        for (int m = 0; m < 16; ++m) {
-          const int k1 = S2 * m + hh;
-          Pab[SNS_IDX(M * j + (k1 ^ j), N)] = cmul(v[m], tw(m));  // four-step twiddle W_N^(j k1)
+          for (int m = 0; m < NZ; ++m) {
+            const int k1 = S2 * m + hh;
+            Pab[SNS_IDX(pslot(j, k1, rB), N)] = cmul(v[m], twhalf(m));  // W_N^(j k1) / 2
+          }
         }
       }
       __syncwarp();
@@ -966,14 +1003,14 @@ k_xpass_w(float2* __restrict__ work, const float2* __restrict__ unyq, const floa
       // ---- forward stage B, r2c unpack through the partner lane, stores to HBM
       {
         const int k1 = lane % M, r = lane / M;
-        const int partner = (N == 512) ? ((32 - lane) & 31) : ((lane & 16) + ((16 - k1) & 15));
+        const int partner = (N == 512) ? ((32 - lane) & 31) : ((lane & ~(M - 1)) + ((M - k1) & (M - 1)));
         const long long row = it * R + r;
 #pragma unroll 1
         for (int ab = 3 * half; ab < 3 * half + 3; ++ab) {
           const C* Pab = Wc + ((ab % 3) * R + r) * N;
           C v[16];
 #pragma unroll
-          for (int jj = 0; jj < 16; ++jj) v[jj] = Pab[SNS_IDX(M * jj + (k1 ^ jj), N)];
+          for (int jj = 0; jj < 16; ++jj) v[jj] = Pab[SNS_IDX(pslot(jj, k1, r), N)];
           dft16<-1, C, true>(v);  // v[i] = X(k1 + M i)
           C* o0 = work + (long long)(2 * ab) * g.field + row * g.pitch;
           C* o1 = o0 + g.field;
@@ -984,8 +1021,9 @@ k_xpass_w(float2* __restrict__ work, const float2* __restrict__ unyq, const floa
             const C zm = shfl2(send, partner);  // X(N - k1 - M i)
             const int kk = k1 + M * i;
             if (kk <= NH) {
-              C A, B;
-              unpack_pair(v[i], zm, &A, &B);
+              // r2c unpack of the halved transform: A = X(k) + conj X(N-k), B = -i (X(k) - conj X(N-k))
+              const C sm = padd(v[i], zm), df = psub(v[i], zm);
+              const C A = cmk(sm.x, df.y), B = cmk(sm.y, -df.x);
               o0[SNS_IDX(kk, g.pitch)] = A;
               o1[SNS_IDX(kk, g.pitch)] = B;
               if (kk == NH) {
@@ -2163,7 +2201,7 @@ struct Launch {
   }
   static void xpass2(void* work, const void* unyq, const void* phase, double scale, int nyq_scalar, double* nyq_part,
                      const void* tw2, Geom g, int grid, int* err, cudaStream_t st) {
-    if constexpr ((N == 256 || N == 512) && std::is_same_v<C, float2>) {
+    if constexpr ((N == 128 || N == 256 || N == 512) && std::is_same_v<C, float2>) {
       k_xpass_w<N><<<grid, 32 * XW<N>::WARPS, XW<N>::smem, st>>>(F(work), F(unyq), F(phase), scale, nyq_scalar,
                                                                  nyq_part, F(tw2), g, err);
     } else if constexpr (N == 256 || N == 512) {
@@ -2208,7 +2246,7 @@ struct Launch {
   }
   // Persistent grid of the two-stage x pass (0: this size uses the generic x pass).
   static int xpass2_grid(int nsm) {
-    if constexpr ((N == 256 || N == 512) && std::is_same_v<C, float2>) {
+    if constexpr ((N == 128 || N == 256 || N == 512) && std::is_same_v<C, float2>) {
       int nb = 0;
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_xpass_w<N>, 32 * XW<N>::WARPS, XW<N>::smem);
       // every warp owns row groups: no CTA beyond one per XW::WARPS row groups
@@ -2281,7 +2319,7 @@ struct Launch {
   }
   // Opt every kernel of this size into its dynamic shared memory (once per process).
   static void init() {
-    if constexpr ((N == 256 || N == 512) && std::is_same_v<C, float2>) set_smem(k_xpass_w<N>, XW<N>::smem);
+    if constexpr ((N == 128 || N == 256 || N == 512) && std::is_same_v<C, float2>) set_smem(k_xpass_w<N>, XW<N>::smem);
     else if constexpr (N == 256 || N == 512) set_smem(k_xpass2<N, C>, XP<N, C>::smem);
     if constexpr (N == 128 || N == 256 || N == 512) set_smem(k_p5<N, C>, tma_smem<N, C>());
     set_smem(k_yz_tma<N, 2, +1, 1, C>, tma_smem<N, C>());
