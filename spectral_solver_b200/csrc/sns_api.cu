@@ -523,7 +523,8 @@ void velocity_partials(sns_handle* h) {
             h->tma_grid, h->stream);
   o->yz_tma(h->map_work_y, 1, +1, 0, tma_args(h, 0, 3, tiles, h->work, 0, 1.0), h->tw, h->phase, g, h->tma_grid,
             h->stream);
-  o->xpass_diag(h->work, h->u(), h->inv_size(), h->nyq_clean ? 1 : 0, h->partials, h->tw, g, h->stream);
+  o->xpass_diag2(h->work, h->u(), h->inv_size(), h->nyq_clean ? 1 : 0, h->partials, h->tw, h->tw2, g, h->x2_grid,
+                 h->err_word, h->stream);
 }
 
 // The same reduced: energy sum in h->red[0], vmax^2 in h->red[1].

@@ -798,7 +798,11 @@ struct XW {
   static_assert(R * M == 32, "a warp covers its rows' lanes");
 };
 
-template <int N>
+// DIAG: the physical velocity's per-row energy and vmax^2 instead (the inverse stages only):
+// work fields 0..2 hold u_0..u_2 on one grid after the inverse z and y passes; the two packed
+// sequences u_0 + i u_1 and u_2 meet in registers and each row's sum of |u|^2 / 2 and max of
+// |u|^2 go to part[2 row], part[2 row + 1] (what k_xpass_diag writes).
+template <int N, bool DIAG = false>
 __global__ void __launch_bounds__(32 * XW<N>::WARPS, 1)
 k_xpass_w(float2* __restrict__ work, const float2* __restrict__ unyq, const float2* __restrict__ phase, double scale,
           int nyq_scalar, double* __restrict__ nyq_part, const float2* __restrict__ tw2_g, Geom g, int* err) {
@@ -825,13 +829,15 @@ k_xpass_w(float2* __restrict__ work, const float2* __restrict__ unyq, const floa
   __syncwarp();
   const long long niter = (long long)N * N / R;
   const long long gw = (long long)blockIdx.x * X::WARPS + warp, nw = (long long)gridDim.x * X::WARPS;
+  constexpr int NF = DIAG ? 3 : 6;  // staged fields per row
+  constexpr int NC = DIAG ? 2 : 3;  // complex sequences per row (packed pairs of real fields)
   auto issue = [&](long long it) {
-    mbar_arrive_expect_tx(bar, R * 6 * X::kRowBytes);
+    mbar_arrive_expect_tx(bar, R * NF * X::kRowBytes);
 #pragma unroll
     for (int r = 0; r < R; ++r) {
       const long long row = it * R + r;
 #pragma unroll
-      for (int f = 0; f < 6; ++f)
+      for (int f = 0; f < NF; ++f)
         bulk_load(stg + (r * 6 + f) * RS, work + (long long)f * g.field + SNS_IDX(row, (long long)N * N) * g.pitch,
                   X::kRowBytes, bar);
     }
@@ -880,32 +886,39 @@ k_xpass_w(float2* __restrict__ work, const float2* __restrict__ unyq, const floa
     {
       const int t = lane % M, r = lane / M;
 #pragma unroll 1
-      for (int c = 0; c < 3; ++c) {
+      for (int c = 0; c < NC; ++c) {
         const C* Ur = stg + (r * 6 + 2 * c) * RS;
         const C* Vr = Ur + RS;
+        const bool has_v = !(DIAG && c == 1);  // the diagnostic's second sequence is u_2 alone
         C v[16];
 #pragma unroll
         for (int q = 0; q < 16; ++q) {
           // x = t + M q: below N/2 for q < 8, N/2 + t for q = 8, above N/2 for q > 8
           const int x = t + M * q;
           C z;
+          const C zero = cmk(0.f, 0.f);
           if (q == 0 && t == 0) {
-            z = cmk(Ur[0].x, Vr[0].x);
+            z = cmk(Ur[0].x, has_v ? Vr[0].x : 0.f);
           } else if (q < 8) {
-            const C U = Ur[SNS_IDX(x, RS)], V = Vr[SNS_IDX(x, RS)];
+            const C U = Ur[SNS_IDX(x, RS)], V = has_v ? Vr[SNS_IDX(x, RS)] : zero;
             z = cmk(U.x - V.y, U.y + V.x);
           } else if (q == 8 && t == 0) {
             C U, V;
             if (nyq_scalar) {
-              U = cscale(unyq[(long long)c * g.field + NH], (float)scale);
-              V = cmul(U, phase[NH + 3 * N / 2]);
+              if constexpr (DIAG) {
+                U = cscale(unyq[(long long)(2 * c) * g.field + NH], (float)scale);
+                V = has_v ? cscale(unyq[(long long)(2 * c + 1) * g.field + NH], (float)scale) : zero;
+              } else {
+                U = cscale(unyq[(long long)c * g.field + NH], (float)scale);
+                V = cmul(U, phase[NH + 3 * N / 2]);
+              }
             } else {
               U = Ur[NH];
-              V = Vr[NH];
+              V = has_v ? Vr[NH] : zero;
             }
             z = cmk(U.x, V.x);
           } else {
-            const C U = Ur[SNS_IDX(N - x, RS)], V = Vr[SNS_IDX(N - x, RS)];
+            const C U = Ur[SNS_IDX(N - x, RS)], V = has_v ? Vr[SNS_IDX(N - x, RS)] : zero;
             z = cmk(U.x + V.y, V.x - U.y);
           }
           v[q] = z;
@@ -927,12 +940,12 @@ k_xpass_w(float2* __restrict__ work, const float2* __restrict__ unyq, const floa
     constexpr int MP = (N == 128) ? 2 : 1;
     constexpr int NZ = 16 / MP;  // positions per lane and row
     auto row_b = [&](int p) { return N == 512 ? 0 : (N == 256 ? (lane >> 4) : 2 * p + (lane >> 4)); };
-    C z[MP][3][NZ];
+    C z[MP][3][NZ];  // (the diagnostic uses the first two)
 #pragma unroll
     for (int p = 0; p < MP; ++p) {
       const int rB = row_b(p);
 #pragma unroll
-      for (int c = 0; c < 3; ++c) {
+      for (int c = 0; c < NC; ++c) {
         const C* W = Wc + (rB * 3 + c) * N;
         C v[NZ];
 #pragma unroll
@@ -963,8 +976,35 @@ k_xpass_w(float2* __restrict__ work, const float2* __restrict__ unyq, const floa
     }
     __syncwarp();  // Wc is read; the products overwrite it
 
+    if constexpr (DIAG) {
+      // |u|^2 = (u_0 + i u_1) magnitude^2 + u_2^2 per position, in FP64; a row's lanes are
+      // the whole warp (N = 512) or one half-warp per row (N = 256, and each pass at 128)
 #pragma unroll
-    for (int half = 0; half < 2; ++half) {
+      for (int p = 0; p < MP; ++p) {
+        double es = 0.0, vm = 0.0;
+#pragma unroll
+        for (int q = 0; q < NZ; ++q) {
+          const double ax = z[p][0][q].x, ay = z[p][0][q].y, bx = z[p][1][q].x;
+          const double s2 = ax * ax + ay * ay + bx * bx;
+          es += 0.5 * s2;
+          vm = fmax(vm, s2);
+        }
+#pragma unroll
+        for (int o = (N == 512 ? 16 : 8); o > 0; o >>= 1) {
+          es += __shfl_xor_sync(kFull, es, o);
+          vm = fmax(vm, __shfl_xor_sync(kFull, vm, o));
+        }
+        if ((lane & (N == 512 ? 31 : 15)) == 0) {
+          const long long row = it * R + row_b(p);
+          nyq_part[SNS_IDX(2 * row, 2LL * N * N)] = es;
+          nyq_part[SNS_IDX(2 * row + 1, 2LL * N * N)] = vm;
+        }
+      }
+      __syncwarp();  // Wc is read; the next row group's inverse stage A overwrites it
+    }
+
+#pragma unroll
+    for (int half = 0; half < (DIAG ? 0 : 2); ++half) {
       // ---- products and forward stage A: P[ab % 3][j][k1] in Wc at pslot(j, k1, row)
 #pragma unroll
       for (int p = 0; p < MP; ++p) {
@@ -1038,6 +1078,7 @@ k_xpass_w(float2* __restrict__ work, const float2* __restrict__ unyq, const floa
     }
   }
   if (!ok && lane == 0) atomicExch(err, kErrTmaTimeout);
+  if constexpr (DIAG) return;
   // per-CTA Nyquist partials, fixed order: [field][cta]
   __syncthreads();
   if (tid < 12) {
@@ -2264,6 +2305,23 @@ struct Launch {
       return 0;
     }
   }
+  // physical energy / vmax^2 per row: the warp-per-row kernel where it exists (FP32, N = 128,
+  // 256, 512; grid as the x pass's), else the generic one-row-per-CTA kernel
+  static void xpass_diag2(const void* work, const void* unyq, double scale, int nyq_scalar, double* partials,
+                          const void* tw, const void* tw2, Geom g, int grid, int* err, cudaStream_t st) {
+    if constexpr ((N == 128 || N == 256 || N == 512) && std::is_same_v<C, float2>) {
+      if (grid > 0) {
+        k_xpass_w<N, true><<<grid, 32 * XW<N>::WARPS, XW<N>::smem, st>>>(
+            static_cast<float2*>(const_cast<void*>(work)), F(unyq), nullptr, scale, nyq_scalar, partials, F(tw2), g,
+            err);
+        return;
+      }
+    }
+    (void)tw2;
+    (void)grid;
+    (void)err;
+    xpass_diag(work, unyq, scale, nyq_scalar, partials, tw, g, st);
+  }
   static void omega_hat(const void* u, void* w, Geom g, cudaStream_t st) {
     const long long total = (long long)N * N * (N / 2 + 1);
     k_omega_hat<C><<<(unsigned)((total + 255) / 256), 256, 0, st>>>(F(u), F(w), g);
@@ -2319,7 +2377,10 @@ struct Launch {
   }
   // Opt every kernel of this size into its dynamic shared memory (once per process).
   static void init() {
-    if constexpr ((N == 128 || N == 256 || N == 512) && std::is_same_v<C, float2>) set_smem(k_xpass_w<N>, XW<N>::smem);
+    if constexpr ((N == 128 || N == 256 || N == 512) && std::is_same_v<C, float2>) {
+      set_smem(k_xpass_w<N>, XW<N>::smem);
+      set_smem(k_xpass_w<N, true>, XW<N>::smem);
+    }
     else if constexpr (N == 256 || N == 512) set_smem(k_xpass2<N, C>, XP<N, C>::smem);
     if constexpr (N == 128 || N == 256 || N == 512) set_smem(k_p5<N, C>, tma_smem<N, C>());
     set_smem(k_yz_tma<N, 2, +1, 1, C>, tma_smem<N, C>());
@@ -2341,7 +2402,7 @@ struct Launch {
   static const Ops* table() {
     static const Ops ops = {N,  (int)sizeof(C), kT, init, zpass_inv_phase, ypass, zpass, xpass_products, nyq_reduce,
                             sweep, xpass_r2c, xpass_c2r, xpass_diag, yz_tma, tma_blocks_per_sm, xpass2, xpass2_grid,
-                            p5, p5_grid, omega_hat, xpass_rot, sweep_rot};
+                            p5, p5_grid, omega_hat, xpass_rot, sweep_rot, xpass_diag2};
     return &ops;
   }
 };

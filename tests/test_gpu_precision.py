@@ -60,7 +60,7 @@ def test_fp32_rhs_matches_oracle(Solver, n):
     assert rel_l2(r, r_ref) < 2e-5
 
 
-@pytest.mark.parametrize("n", [32, 48, 96, 128])
+@pytest.mark.parametrize("n", [32, 48, 96, 128, 256])
 def test_fp32_diagnostics_match_oracle(Solver, n):
     """Energy, enstrophy, dissipation and vmax of an FP32 state against the FP64 oracle
     (the FP32 rounding of the state bounds the relative error: 1e-6)."""
