@@ -456,15 +456,15 @@ void step_once(sns_handle* h, double dt) {
   }
 }
 
-void velocity_partials(sns_handle* h);
+int velocity_partials(sns_handle* h);
 
 // One step with the adaptive CFL rule on the device: vmax of the current state (the same
 // per-row partials as sns_max_velocity; their max and the clock's next step in one launch),
 // then the three stages on that step.  Nothing here waits for the host, so the step can be
 // captured into a graph.
 void step_on_clock(sns_handle* h) {
-  velocity_partials(h);
-  sns::launch_clock_step_partials(h->partials + 1, h->n * h->n, 2, h->clock, h->stream);
+  const int pairs = velocity_partials(h);
+  sns::launch_clock_step_partials(h->partials + 1, pairs, 2, h->clock, h->stream);
   h->on_clock = true;
   try {
     step_once(h, 0.0);
@@ -514,8 +514,9 @@ void download_full(sns_handle* h, const void* src, double* host, const sns::Comp
 }
 
 // Physical velocity of the state: inverse z and y passes of u without the phase shift, then
-// the diagnostic x pass; per-row (energy, vmax^2) partials in h->partials.
-void velocity_partials(sns_handle* h) {
+// the diagnostic x pass; (energy, vmax^2) partials in h->partials, per row or per CTA of the
+// warp-per-row kernel; returns how many pairs.
+int velocity_partials(sns_handle* h) {
   const sns::Ops* o = h->ops;
   const sns::Geom& g = h->g;
   const int tiles = h->nyq_clean ? h->tiles_data() : h->tiles_all();
@@ -523,14 +524,13 @@ void velocity_partials(sns_handle* h) {
             h->tma_grid, h->stream);
   o->yz_tma(h->map_work_y, 1, +1, 0, tma_args(h, 0, 3, tiles, h->work, 0, 1.0), h->tw, h->phase, g, h->tma_grid,
             h->stream);
-  o->xpass_diag2(h->work, h->u(), h->inv_size(), h->nyq_clean ? 1 : 0, h->partials, h->tw, h->tw2, g, h->x2_grid,
-                 h->err_word, h->stream);
+  return o->xpass_diag2(h->work, h->u(), h->inv_size(), h->nyq_clean ? 1 : 0, h->partials, h->tw, h->tw2, g,
+                        h->x2_grid, h->err_word, h->stream);
 }
 
 // The same reduced: energy sum in h->red[0], vmax^2 in h->red[1].
 void velocity_reductions(sns_handle* h) {
-  velocity_partials(h);
-  const int rows = h->n * h->n;
+  const int rows = velocity_partials(h);  // (energy, vmax^2) pairs
   sns::launch_reduce(h->partials, rows, 2, 0, h->red + 0, h->stream);
   sns::launch_reduce(h->partials + 1, rows, 2, 1, h->red + 1, h->stream);
 }

@@ -798,10 +798,11 @@ struct XW {
   static_assert(R * M == 32, "a warp covers its rows' lanes");
 };
 
-// DIAG: the physical velocity's per-row energy and vmax^2 instead (the inverse stages only):
-// work fields 0..2 hold u_0..u_2 on one grid after the inverse z and y passes; the two packed
-// sequences u_0 + i u_1 and u_2 meet in registers and each row's sum of |u|^2 / 2 and max of
-// |u|^2 go to part[2 row], part[2 row + 1] (what k_xpass_diag writes).
+// DIAG: the physical velocity's energy and vmax^2 instead (the inverse stages only): work
+// fields 0..2 hold u_0..u_2 on one grid after the inverse z and y passes; the two packed
+// sequences u_0 + i u_1 and u_2 meet in registers, each row's sum of |u|^2 / 2 and max of
+// |u|^2 are reduced over its lanes, and the CTA's totals (rows in a fixed order per warp,
+// warps in order) go to part[2 cta], part[2 cta + 1].
 template <int N, bool DIAG = false>
 __global__ void __launch_bounds__(32 * XW<N>::WARPS, 1)
 k_xpass_w(float2* __restrict__ work, const float2* __restrict__ unyq, const float2* __restrict__ phase, double scale,
@@ -875,6 +876,7 @@ k_xpass_w(float2* __restrict__ work, const float2* __restrict__ unyq, const floa
 
   bool ok = true;
   int k = 0;
+  double acc_es = 0.0, acc_vm = 0.0;  // DIAG: running totals of this lane's rows
   for (long long it = gw; it < niter; it += nw, ++k) {
     const bool landed = mbar_wait_bounded(bar, (uint32_t)k & 1u);
     if (!__all_sync(kFull, landed)) {  // the copy of this row group never landed; none other is in flight
@@ -994,11 +996,8 @@ k_xpass_w(float2* __restrict__ work, const float2* __restrict__ unyq, const floa
           es += __shfl_xor_sync(kFull, es, o);
           vm = fmax(vm, __shfl_xor_sync(kFull, vm, o));
         }
-        if ((lane & (N == 512 ? 31 : 15)) == 0) {
-          const long long row = it * R + row_b(p);
-          nyq_part[SNS_IDX(2 * row, 2LL * N * N)] = es;
-          nyq_part[SNS_IDX(2 * row + 1, 2LL * N * N)] = vm;
-        }
+        acc_es += es;  // every lane of the row holds the row's totals
+        acc_vm = fmax(acc_vm, vm);
       }
       __syncwarp();  // Wc is read; the next row group's inverse stage A overwrites it
     }
@@ -1078,7 +1077,30 @@ k_xpass_w(float2* __restrict__ work, const float2* __restrict__ unyq, const floa
     }
   }
   if (!ok && lane == 0) atomicExch(err, kErrTmaTimeout);
-  if constexpr (DIAG) return;
+  if constexpr (DIAG) {
+    // one lane per row group: lane 0 (N = 512: the warp is one row), lanes 0 and 16 otherwise
+    double w_es = acc_es, w_vm = acc_vm;
+    if constexpr (N != 512) {
+      w_es = __shfl_sync(kFull, acc_es, 0) + __shfl_sync(kFull, acc_es, 16);
+      w_vm = fmax(__shfl_sync(kFull, acc_vm, 0), __shfl_sync(kFull, acc_vm, 16));
+    }
+    if (lane == 0) {
+      s_nyq[2 * warp] = w_es;
+      s_nyq[2 * warp + 1] = w_vm;
+    }
+    __syncthreads();
+    if (tid == 0) {
+      double es = 0.0, vm = 0.0;
+#pragma unroll 1
+      for (int w = 0; w < X::WARPS; ++w) {
+        es += s_nyq[2 * w];
+        vm = fmax(vm, s_nyq[2 * w + 1]);
+      }
+      nyq_part[2 * blockIdx.x] = es;
+      nyq_part[2 * blockIdx.x + 1] = vm;
+    }
+    return;
+  }
   // per-CTA Nyquist partials, fixed order: [field][cta]
   __syncthreads();
   if (tid < 12) {
@@ -2307,20 +2329,21 @@ struct Launch {
   }
   // physical energy / vmax^2 per row: the warp-per-row kernel where it exists (FP32, N = 128,
   // 256, 512; grid as the x pass's), else the generic one-row-per-CTA kernel
-  static void xpass_diag2(const void* work, const void* unyq, double scale, int nyq_scalar, double* partials,
-                          const void* tw, const void* tw2, Geom g, int grid, int* err, cudaStream_t st) {
+  static int xpass_diag2(const void* work, const void* unyq, double scale, int nyq_scalar, double* partials,
+                         const void* tw, const void* tw2, Geom g, int grid, int* err, cudaStream_t st) {
     if constexpr ((N == 128 || N == 256 || N == 512) && std::is_same_v<C, float2>) {
       if (grid > 0) {
         k_xpass_w<N, true><<<grid, 32 * XW<N>::WARPS, XW<N>::smem, st>>>(
             static_cast<float2*>(const_cast<void*>(work)), F(unyq), nullptr, scale, nyq_scalar, partials, F(tw2), g,
             err);
-        return;
+        return grid;  // one (energy, vmax^2) pair per CTA
       }
     }
     (void)tw2;
     (void)grid;
     (void)err;
     xpass_diag(work, unyq, scale, nyq_scalar, partials, tw, g, st);
+    return N * N;  // one pair per row
   }
   static void omega_hat(const void* u, void* w, Geom g, cudaStream_t st) {
     const long long total = (long long)N * N * (N / 2 + 1);

@@ -124,9 +124,10 @@ struct Ops {
   void (*sweep_rot)(const void* work, void* u, void* gbuf, void* rhs, const double* nyq_sums, const void* phase,
                     SweepArgs a, Geom g, cudaStream_t st);
   // xpass_diag on the warp-per-row x pass where the handle runs it (FP32, N = 128, 256, 512;
-  // grid = its x-pass grid, > 0), else xpass_diag; tw2 as for xpass2
-  void (*xpass_diag2)(const void* work, const void* unyq, double scale, int nyq_scalar, double* partials,
-                      const void* tw, const void* tw2, Geom g, int grid, int* err, cudaStream_t st);
+  // grid = its x-pass grid, > 0: one (energy, vmax^2) pair per CTA), else xpass_diag (one pair
+  // per row); returns the number of pairs written; tw2 as for xpass2
+  int (*xpass_diag2)(const void* work, const void* unyq, double scale, int nyq_scalar, double* partials,
+                     const void* tw, const void* tw2, Geom g, int grid, int* err, cudaStream_t st);
 };
 
 // nullptr when the size has no FFT plan; precision 0 = FP64, 1 = FP32
