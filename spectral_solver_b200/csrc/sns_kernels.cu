@@ -2188,22 +2188,30 @@ __global__ void __launch_bounds__(256) k_spectral_diag(const C* __restrict__ u, 
 }
 
 // Fixed-order reduction of `count` partials at stride `stride` (one CTA).
-__global__ void __launch_bounds__(256) k_reduce(const double* __restrict__ partials, int count, int stride,
-                                                int op_max, double* __restrict__ out) {
-  __shared__ double red[256];
-  double s = 0.0;
-  for (int i = threadIdx.x; i < count; i += 256) {
-    const double v = partials[(long long)i * stride];
-    s = op_max ? fmax(s, v) : s + v;
+// One CTA of 1024 threads; four independent loads in flight per thread (the partials are
+// read once, a few MB at most), then a fixed-order tree: the result does not depend on timing.
+__global__ void __launch_bounds__(1024) k_reduce(const double* __restrict__ partials, int count, int stride,
+                                                 int op_max, double* __restrict__ out) {
+  __shared__ double red[1024];
+  const int tid = threadIdx.x;
+  double s[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int i0 = tid; i0 < count; i0 += 4 * 1024) {
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int i = i0 + u * 1024;
+      if (i < count) {
+        const double v = partials[(long long)i * stride];
+        s[u] = op_max ? fmax(s[u], v) : s[u] + v;
+      }
+    }
   }
-  red[threadIdx.x] = s;
+  red[tid] = op_max ? fmax(fmax(s[0], s[1]), fmax(s[2], s[3])) : (s[0] + s[1]) + (s[2] + s[3]);
   __syncthreads();
-  for (int o = 128; o > 0; o >>= 1) {
-    if (threadIdx.x < o) red[threadIdx.x] = op_max ? fmax(red[threadIdx.x], red[threadIdx.x + o])
-                                                   : red[threadIdx.x] + red[threadIdx.x + o];
+  for (int o = 512; o > 0; o >>= 1) {
+    if (tid < o) red[tid] = op_max ? fmax(red[tid], red[tid + o]) : red[tid] + red[tid + o];
     __syncthreads();
   }
-  if (threadIdx.x == 0) *out = red[0];
+  if (tid == 0) *out = red[0];
 }
 
 // ------------------------------------------------------------------------------------
@@ -2543,26 +2551,33 @@ void launch_clock_step(const double* vmax2, double* clock, cudaStream_t st) {
 
 // The max of the per-row vmax^2 partials (as k_reduce: max is exact in any order) and the
 // clock's step from it in one launch, for the device CFL step.
-__global__ void __launch_bounds__(256) k_clock_step_partials(const double* __restrict__ partials, int count,
-                                                             int stride, double* __restrict__ c) {
-  __shared__ double red[256];
-  double m = 0.0;
-  for (int i = threadIdx.x; i < count; i += 256) m = fmax(m, partials[(long long)i * stride]);
-  red[threadIdx.x] = m;
+__global__ void __launch_bounds__(1024) k_clock_step_partials(const double* __restrict__ partials, int count,
+                                                              int stride, double* __restrict__ c) {
+  __shared__ double red[1024];
+  const int tid = threadIdx.x;
+  double m[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int i0 = tid; i0 < count; i0 += 4 * 1024) {
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int i = i0 + u * 1024;
+      if (i < count) m[u] = fmax(m[u], partials[(long long)i * stride]);
+    }
+  }
+  red[tid] = fmax(fmax(m[0], m[1]), fmax(m[2], m[3]));
   __syncthreads();
-  for (int o = 128; o > 0; o >>= 1) {
-    if (threadIdx.x < o) red[threadIdx.x] = fmax(red[threadIdx.x], red[threadIdx.x + o]);
+  for (int o = 512; o > 0; o >>= 1) {
+    if (tid < o) red[tid] = fmax(red[tid], red[tid + o]);
     __syncthreads();
   }
-  if (threadIdx.x == 0) clock_advance(red, c);
+  if (tid == 0) clock_advance(red, c);
 }
 
 void launch_clock_step_partials(const double* partials, int count, int stride, double* clock, cudaStream_t st) {
-  k_clock_step_partials<<<1, 256, 0, st>>>(partials, count, stride, clock);
+  k_clock_step_partials<<<1, 1024, 0, st>>>(partials, count, stride, clock);
 }
 
 void launch_reduce(const double* partials, int count, int stride, int op_max, double* out, cudaStream_t st) {
-  k_reduce<<<1, 256, 0, st>>>(partials, count, stride, op_max, out);
+  k_reduce<<<1, 1024, 0, st>>>(partials, count, stride, op_max, out);
 }
 
 }  // namespace sns
