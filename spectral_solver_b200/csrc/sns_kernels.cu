@@ -772,7 +772,8 @@ k_xpass2(C* __restrict__ work, const C* __restrict__ unyq, const C* __restrict__
 //                    registers
 //   products + forward stage A  per product u_a u_b (both grids: real and imaginary part)
 //                    the M-point DFT over n at fixed j (at N = 512 split in frequency: one
-//                    shuffle, then a 16-point DFT), times W_N^(j k1); out to P[ab][j][k1]
+//                    shuffle, then a 16-point DFT; at N = 128 an 8-point DFT), times
+//                    W_N^(j k1) / 2 (the r2c unpack's factor 1/2, exact); out to P[ab][j][k1]
 //   forward stage B  lane k1: the 16-point DFT over j, outputs k1 + M k2; r2c unpack of the
 //                    two grids through the partner lane (N - k), 128-byte stores to HBM
 // The products run in two halves of three (00 01 02, then 11 12 22), each through Wc and its
