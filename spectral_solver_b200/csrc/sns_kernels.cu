@@ -413,8 +413,9 @@ k_xpass_products(C* __restrict__ work, const C* __restrict__ unyq, const C* __re
 
 
 // ------------------------------------------------------------------------------------
-// P3 for N = 256 (16 x 16) and N = 512 (16 x 32): two-stage FFTs with one shared-memory
-// round trip each.  Persistent CTAs; the 6 input rows of the next row group arrive by
+// P3 of the FP64 form for N = 256 (16 x 16) and N = 512 (16 x 32; the FP32 form runs
+// k_xpass_w below): two-stage FFTs with one shared-memory round trip each.  Persistent CTAs;
+// the 6 input rows of the next row group arrive by
 // cp.async.bulk into a second staging buffer while the current group is transformed.
 //   inverse stage A : radix 16 over stride-M inputs, the packing Z = U + iV (with the
 //                     mirror and the real-part rule at mx = 0, N/2) fused into the loads
@@ -434,15 +435,14 @@ struct XP {
   static constexpr int M = N / 16;                 // stage-B radix
   static constexpr bool PAIR = (M == 32);          // radix 32 as two radix-16 halves + shuffle
   static constexpr int NH = N / 2;
-  // rows per iteration: two where their staging fits the CTA budget (N = 256; N = 512 in
-  // FP32), so one barrier sequence serves two rows and, at N = 512, the inverse stages keep
-  // all 192 threads busy (96 at N = 256, one half-warp per FFT)
-  static constexpr int ROWS = (N == 256 || sizeof(C) == 8) ? 2 : 1;
+  // rows per iteration: two where their staging fits the CTA budget at two CTAs per SM
+  // (N = 256), so one barrier sequence serves two rows; at N = 512 one (two rows, all six
+  // warps busy in the inverse stages but one CTA per SM, measured slower)
+  static constexpr int ROWS = (N == 256) ? 2 : 1;
   static constexpr int SP = N + N / 16;            // padded sequence (one slot per 16)
   static constexpr int NT = 192;
-  // resident CTAs per SM the register budget is built for: the FP32 rows are half the
-  // shared memory, so three CTAs fit where FP64 fits two
-  static constexpr int MINB = (sizeof(C) == 8 && N == 256) ? 3 : 2;
+  // resident CTAs per SM the register budget is built for
+  static constexpr int MINB = 2;
   // staged row of one field: NH + 1 values rounded up to 16 bytes (the bulk-copy unit)
   static constexpr int RS = (int)(((NH + 1) * sizeof(C) + 15) / 16 * 16 / sizeof(C));
   static constexpr int ROWIN = 6 * RS;
@@ -516,26 +516,8 @@ k_xpass2(C* __restrict__ work, const C* __restrict__ unyq, const C* __restrict__
   };
   if (tid == 0 && blockIdx.x < niter) issue(blockIdx.x, 0);
   // Stage-B twiddles W_N^(j*rr), rr = 2 i + h: the same for every row this thread transforms
-  // (inverse and forward stages B share the lane mapping).  In the FP32 form with the radix-32
-  // split they come from 8 values held in registers, W^(j (h + 2 c)) * W^(8 j a) with
-  // i = 4 a + c, instead of 16 shared-memory loads per FFT (the x pass is bound by its
-  // shared-memory pipe); the FP64 form has no registers to spare and loads them.
-  constexpr bool kTwReg = X::PAIR && sizeof(C) == 8;
-  C twP[4], twQ[4];
-  if constexpr (kTwReg) {
-    const int j = tid & 15, h = (tid >> 4) & 1;
-#pragma unroll
-    for (int c = 0; c < 4; ++c) twP[c] = tw2[(h + 2 * c) * 16 + j];
-#pragma unroll
-    for (int a = 0; a < 4; ++a) twQ[a] = tw2[8 * a * 16 + j];
-  }
-  auto stage_b_tw = [&](int i, int j, int h) -> C {
-    if constexpr (kTwReg) {
-      return i < 4 ? twP[i] : cmul(twP[i & 3], twQ[i >> 2]);
-    } else {
-      return tw2[(2 * i + h) * 16 + j];
-    }
-  };
+  // (inverse and forward stages B share the lane mapping), from the shared table.
+  auto stage_b_tw = [&](int i, int j, int h) -> C { return tw2[(2 * i + h) * 16 + j]; };
   double nyq_p0 = 0.0, nyq_ps = 0.0;  // owned by the lane that holds k = N/2 of its pair
   int k = 0;
   for (long long it = blockIdx.x; it < niter; ++k, it += gridDim.x) {
